@@ -1,0 +1,347 @@
+"""Benchmark of the fused FP64 RK4 stepper (headline: DOF-stages/s at p=3).
+
+Workload: the isentropic vortex (reference IC) on the 10x10 periodic domain,
+768x768 cells = 1,179,648 triangles, p=3 (10 nodes), integration_order=10,
+perturb_grid=0.2, RK4 with dt=1.4e-5. A step is one RK4 step over all
+elements; one DOF-stage is one element node (4 conserved components) advanced
+through one RK stage, so a step is K*Np*4 DOF-stages.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the reference's own CPU code (oracle/_ref, the
+reference compiled from its sources with -O2 -fopenmp) with all host threads on
+a bounded sample of the same per-element work. With N>1 (torchrun) every rank
+advances its own replica (the problem does not need a collective); rank 0
+prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 768
+P, IO, PERTURB, DT = 3, 10, 0.2, 1.4e-5
+NP = (P + 1) * (P + 2) // 2
+# Algorithmic HBM bytes per DOF-stage of the 3-register RK4 scheme: 16 state
+# vectors of 4 doubles over 4 stages (128 B) plus per-element geometry and
+# connectivity (124 B per element, i.e. 124/Np per node).
+B_ALG = 128.0 + 124.0 / NP
+WORKLOAD = (f"isentropic vortex, {NX}x{NY} cells ({2 * NX * NY:,} triangles), p={P}, "
+            f"integration_order={IO}, perturb_grid={PERTURB}, RK4 dt={DT}")
+METRIC = "FP64 DOF-stages/s p=3"
+UNIT = "DOF-stages/s"
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "vt_ref_harness")
+CPU_SAMPLE_CELLS = 256  # 131,072 triangles, the reference's own OpenMP performance mesh size
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per stage launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_p3_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.dev), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference_harness(cells: int, steps: int, threads: int):
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores",
+               OMP_SCHEDULE="static", OMP_DYNAMIC="false")
+    out = subprocess.run([HARNESS, "--nx", str(cells), "--ny", str(cells), "--p", str(P), "--io",
+                          str(IO), "--perturb", str(PERTURB), "--dt", str(DT), "--steps", str(steps),
+                          "--no-ops", "--time"], env=env, capture_output=True, text=True, check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def cpu_baseline(budget_s: float = 20.0):
+    """The reference's own code timed on this host's cores on a bounded sample."""
+    threads = os.cpu_count() or 1
+    if os.path.exists(HARNESS):
+        cal = run_reference_harness(CPU_SAMPLE_CELLS, 1, threads)
+        per_step = max(cal["stepping_s"], 1e-3)
+        steps = int(max(1, min(50, budget_s / per_step)))
+        r = run_reference_harness(CPU_SAMPLE_CELLS, steps, threads)
+        return {"value": r["dof_stages_per_s"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                "sample": (f"{steps} RK4 steps of the same per-element work (p={P}, io={IO}, perturb "
+                           f"{PERTURB}, dt {DT}) on {CPU_SAMPLE_CELLS}x{CPU_SAMPLE_CELLS} cells "
+                           f"({2 * CPU_SAMPLE_CELLS ** 2:,} triangles); reference -O2 -fopenmp build")}
+    # the C restatement when the reference build is absent
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import vt_oracle
+    vt = import_package()
+    cells = 64
+    pb = vt.Problem(vt.make_params(cells, cells, p=P, integration_order=IO, perturb_grid=PERTURB))
+    om = vt_oracle.OracleMesh(P, pb.array("vertices"), pb.array("conn"), pb.array("type"),
+                              pb.array("minv_ref"), pb.array("stiff_ref"), pb.array("phi_plus"),
+                              pb.array("phi_minus"), pb.array("line_quad"))
+    steps = 5
+    t0 = time.perf_counter()
+    om.step(pb.array("U0"), pb.array("F0"), DT, steps, 1)
+    dt = time.perf_counter() - t0
+    return {"value": pb.K * NP * 4 * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} RK4 steps on {cells}x{cells} cells with the C restatement"}
+
+
+def import_package():
+    import importlib.util
+    name = "vortex_transport_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "vortex-transport_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    if not os.path.exists(HARNESS):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/vt_ref_harness was not built "
+                          "(needs the reference sources at build time)"}))
+        return 0
+    if args.warmup:
+        run_reference_harness(CPU_SAMPLE_CELLS, min(args.warmup, 3), threads)
+    r = run_reference_harness(CPU_SAMPLE_CELLS, args.steps, threads)
+    value = r["dof_stages_per_s"]
+    K_s = 2 * CPU_SAMPLE_CELLS ** 2
+    sample = (f"each step: one RK4 step of the same per-element work (p={P}, io={IO}, perturb "
+              f"{PERTURB}, dt {DT}) on {CPU_SAMPLE_CELLS}x{CPU_SAMPLE_CELLS} cells ({K_s:,} "
+              f"triangles) instead of {NX}x{NY}; reference compiled -O2 -fopenmp")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * r["stepping_s"] / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the reference's isentropic-vortex IC on its generated mesh",
+            "config": {"workload": WORKLOAD, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def b200_arm(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    vt = import_package()
+
+    cells = args.cells
+    workload = WORKLOAD if cells == NX else WORKLOAD.replace(f"{NX}x{NY} cells ({2 * NX * NY:,}",
+                                                             f"{cells}x{cells} cells ({2 * cells * cells:,}")
+    prm = vt.make_params(cells, cells, p=P, integration_order=IO, perturb_grid=PERTURB, time_step=DT)
+    pb = vt.Problem(prm)
+    solver = vt.Solver(pb, device=local)
+    K_el = pb.K
+    dof_stages_per_step = K_el * NP * 4
+    stream = torch.cuda.ExternalStream(solver.stream, device=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not pg:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also captures the step graph)
+    solver.rk4(DT, max(args.warmup, 1))
+
+    # ---- timed region: K steps, state resident in HBM -----------------------
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        solver.rk4_async(DT, args.steps)
+        ev1.record(stream)
+        solver.synchronize()
+        torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    barrier()
+    value = world * dof_stages_per_step * args.steps / (ms * 1e-3)
+
+    # ---- per-stage kernel times (individual launches, events) ---------------
+    stage_ms = solver.profile_stages(DT, 5)
+
+    # ---- end to end through the public API with host buffers -----------------
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
+    host_U = torch.empty((K_el, NP, 4), dtype=torch.float64, pin_memory=True).numpy()
+    host_U[...] = solver.download()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        solver.upload(host_U)  # pinned host -> device
+        vt.rk4(solver, DT, 1)
+        solver.download(out=host_U)  # device -> pinned host
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * dof_stages_per_step * e2e_steps / (e2e_ms * 1e-3) if e2e_steps else None
+    state_bytes = K_el * NP * 4 * 8
+
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        avg_launch_s = ms * 1e-3 / (4 * args.steps)
+        bytes_per_launch = K_el * NP * B_ALG
+        achieved = bytes_per_launch / avg_launch_s / 1e9
+        traffic = profile_traffic()
+        cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the reference's isentropic-vortex IC on its generated mesh",
+            "config": {"workload": workload, "elements": K_el, "nodes_per_element": NP,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (4 resident state vectors of "
+                             f"{state_bytes / 1e6:.0f} MB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_dof_stage": B_ALG,
+                         "note": "achieved = K*Np*B_alg per stage launch / mean launch time in "
+                                 "the timed region (4 launches per step)"},
+            "stage_ms": [float(x) for x in stage_ms],
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
+                    "note": "per step: pinned host U -> device, one RK4 step, device -> host U"},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    solver.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cells", type=int, default=NX, help="cells per side (profiling runs use fewer)")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

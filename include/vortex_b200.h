@@ -1,0 +1,195 @@
+/* vortex_b200: B200-native (sm_100a, FP64) nodal-DG right-hand side and
+ * explicit RK4 / forward-Euler stepper for the 2D compressible Euler equations
+ * on affine triangles, as a drop-in for Vortex-Transport's CPU element loop.
+ *
+ * C ABI only: plain pointers and sizes, no C++ or torch types. Every entry point
+ * returns VT_OK (0) or a status code; nothing in the library calls exit().
+ * A context owns its device memory and one CUDA stream; calls on one context
+ * are serialised by a per-context lock and may come from any host thread.
+ *
+ * Host array layouts follow the reference's nested vectors, flattened
+ * element-major:
+ *   U   K x Np x 4       (rho, rho u, rho v, rho E)   Element.H:30
+ *   F   K x Np x 2 x 4   (x flux, y flux)              Element.H:31
+ * Np = (p+1)(p+2)/2 nodes per element, K = 2 nx ny elements.
+ */
+#ifndef VORTEX_B200_H
+#define VORTEX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define VT_OK 0
+/* The reference's non-physical-state exits (Numericalflux.cpp:42-54, 75-79,
+ * 111-115) become these codes instead of exit(EXIT_FAILURE). */
+#define VT_ERR_NONPHYSICAL_LEFT 1  /* pL <= 0 or rhoL <= 0 */
+#define VT_ERR_NONPHYSICAL_RIGHT 2 /* pR <= 0 or rhoR <= 0 */
+#define VT_ERR_NONPHYSICAL_C2 3    /* Roe-averaged c^2 <= 0 */
+#define VT_ERR_INVALID (-1)        /* bad argument or input file */
+#define VT_ERR_UNSUPPORTED (-2)    /* p, integration order or method out of range */
+#define VT_ERR_CUDA (-3)           /* CUDA runtime error (message in vt_last_message) */
+#define VT_ERR_NO_MEMORY (-4)
+
+/* ---- input file --------------------------------------------------------- */
+/* Mirrors `struct parameters` (Parameters.H:5-19), same fields and types. */
+typedef struct vt_params {
+  int p;
+  float domain_x;
+  float domain_y;
+  int num_element_in_x;
+  int num_element_in_y;
+  float perturb_grid;
+  int integration_order;
+  float simulation_time;
+  int number_time_steps;
+  double time_step;
+  int write_every_steps;
+  int U_initialization_type;
+  int stepping_method;
+} vt_params;
+
+/* Replaces read_input_files (Parameters.cpp:12-64): same `key=value` keys and
+ * std::stoi/stof/stod conversions (so perturb_grid=0.2 reads as 0, as in the
+ * reference); a missing or malformed key returns VT_ERR_INVALID instead of
+ * throwing. */
+int vt_read_input_file(const char* path, vt_params* out);
+int vt_parse_input(const char* text, vt_params* out);
+
+/* Message for the last non-OK status returned on the calling thread. */
+const char* vt_last_message(void);
+
+/* ---- initial condition -------------------------------------------------- */
+/* The isentropic-vortex constants that Element::initialize_hydrodinamics
+ * hard-codes (Element.cpp:134-143), as parameters. */
+typedef struct vt_vortex {
+  double rho_infty, rc, epsilon, gamma, M_infty, p_infty, U_infty, V_infty, x0, y0;
+} vt_vortex;
+
+/* The reference's literals: rho=1, rc=1, eps=0.3, gamma=1.4, M=0.5, p=20/7,
+ * U=V=1/sqrt(2), centre (0,0). */
+void vt_default_vortex(vt_vortex* out);
+
+/* ---- host precompute (main.cpp:99-147) ---------------------------------- */
+typedef struct vt_problem vt_problem;
+
+typedef struct vt_problem_info {
+  int K, p, Np, nfq, nqa, nx, ny;
+} vt_problem_info;
+
+/* Builds the mesh (Meshgeneration.cpp:16-186), quadrature
+ * (Quadraturerule.cpp), reference operators (Preevolve.cpp:15-144),
+ * per-element geometry (Element.cpp:54-116), face tables (Evolve.cpp:76-132)
+ * and the initial state (Element.cpp:119-333). perturb_grid is used as the
+ * float in `prm` (callers wanting the reference's std::stoi quirk go through
+ * vt_read_input_file). ic == NULL uses the reference's vortex. */
+vt_problem* vt_problem_create(const vt_params* prm, const vt_vortex* ic, int* status);
+void vt_problem_destroy(vt_problem* prob);
+int vt_problem_get_info(const vt_problem* prob, vt_problem_info* out);
+
+/* Copies one named array (doubles, or int32 for "conn"/"type") into dst of
+ * `bytes` bytes. Names: vertices, conn, type, nodes_ref, nodes_phys, line_quad,
+ * area_quad, minv_ref, stiff_ref, phi_plus, phi_minus, jac, jinv, detj,
+ * detjinv, normals, sides, U0, F0. */
+int vt_problem_get_array(const vt_problem* prob, const char* name, void* dst, size_t bytes);
+
+/* Nodal flux of a state, the formula the reference applies after every stage
+ * (Timestepping.cpp:141-158). U: K x Np x 4 -> F: K x Np x 2 x 4. */
+int vt_flux_from_state(int K, int p, const double* U, double* F);
+
+/* ---- drop-in boundary: the device solver -------------------------------- */
+/* Everything the reference's Element / Evolve_element objects hold that the
+ * element loop reads (Element.H:19-45, Evolve.H:19-33), as flat host arrays.
+ * The stepper never needs the per-element physical matrices: the elements are
+ * affine, so the reference-space operators plus each element's inverse
+ * Jacobian and determinant carry the same information. */
+typedef struct vt_mesh_desc {
+  int32_t p;                     /* Lagrange order, 0..3 */
+  int32_t n_elements;            /* K */
+  int32_t n_line_points;         /* nfq = gau_integ_line.size(), 1..10 */
+  const int32_t* element_type;   /* K: Element::type */
+  const int32_t* neighbours;     /* K x 3: right, left, vertical element */
+  const double* det_jacobian;    /* K: Element::determinant_jacobian */
+  const double* inv_jacobian;    /* K x 4: Element::inverse_jacobian [00,01,10,11] */
+  const double* normals;         /* K x 3 x 2: outward unit normal per side */
+  const double* side_lengths;    /* K x 3: Element::sides_lenght */
+  const double* inv_mass_ref;    /* Np x Np: inverse_mass_matrix_reference_space */
+  const double* stiffness_ref;   /* 2 x Np x Np: sitffness_matrix_reference_space */
+  const double* line_quadrature; /* nfq x 2: (sigma, weight), gauss_line_integral */
+  const double* phi_plus;        /* 3 x Np x nfq: plus_phi_in_quadrature_points_side_1..3 */
+  const double* phi_minus;       /* 3 x Np x nfq: minus_phi_in_quadrature_points_side_1..3 */
+} vt_mesh_desc;
+
+/* Fills a descriptor whose pointers refer to arrays owned by `prob`. */
+int vt_problem_mesh_desc(const vt_problem* prob, vt_mesh_desc* out);
+
+typedef struct vt_ctx vt_ctx;
+
+/* First failing check of the last step call, in the reference's serial order
+ * (element, then face point, then side, Evolve.cpp:215-221). code 0 = none. */
+typedef struct vt_error_info {
+  int code;
+  int element;
+  int point;
+  int side;
+  int64_t step;  /* 0-based step within the failing call */
+  int stage;     /* 0..3 for RK4, 0 for forward Euler */
+} vt_error_info;
+
+/* Uploads operators and geometry to `device` and allocates the state. Replaces
+ * the per-step work of rk4 / forward_euler (Timestepping.H:8-9). */
+vt_ctx* vt_create(const vt_mesh_desc* desc, int device, int* status);
+void vt_destroy(vt_ctx* ctx);
+
+/* State transfer with host arrays in the reference layout (U: K x Np x 4). */
+int vt_upload_state(vt_ctx* ctx, const double* U);
+/* F (K x Np x 2 x 4) may be NULL; when given it is the nodal flux of U, as the
+ * reference stores it after each step. */
+int vt_download_state(vt_ctx* ctx, double* U, double* F);
+/* Same, with U a device pointer (K x Np x 4, reference layout) on ctx's device. */
+int vt_upload_state_device(vt_ctx* ctx, const double* dU);
+int vt_download_state_device(vt_ctx* ctx, double* dU);
+
+/* nsteps classical RK4 steps (Timestepping.cpp:85-306) / forward-Euler steps
+ * (Timestepping.cpp:39-82) of size dt. Blocks until done and returns VT_OK or
+ * the first non-physical-state code (details via vt_last_error). */
+int vt_step_rk4(vt_ctx* ctx, double dt, int nsteps);
+int vt_step_euler(vt_ctx* ctx, double dt, int nsteps);
+
+/* Same as vt_step_rk4 but only enqueues the work on the context's stream and
+ * returns; vt_synchronize() waits and reports the status. */
+int vt_step_rk4_async(vt_ctx* ctx, double dt, int nsteps);
+int vt_synchronize(vt_ctx* ctx);
+
+/* One right-hand-side evaluation of the current state, DG_time_derivative_U of
+ * evolve_elem (Timestepping.cpp:18-36); Udot is a host K x Np x 4 array. */
+int vt_rhs(vt_ctx* ctx, double* Udot);
+
+int vt_last_error(const vt_ctx* ctx, vt_error_info* out);
+
+/* Simulation time, advanced by dt per step as Element::time is
+ * (Timestepping.cpp:80, :304). */
+double vt_get_time(const vt_ctx* ctx);
+int vt_set_time(vt_ctx* ctx, double t);
+
+/* Conservation totals sum_e detJ_e sum_i W_i U_e,i (W_i = integral of the
+ * i-th basis function), computed on the device. out[4]. */
+int vt_totals(vt_ctx* ctx, double* out);
+
+/* The context's cudaStream_t, for callers that interleave their own work. */
+void* vt_stream(vt_ctx* ctx);
+
+/* Device time of each kernel kind of one RK4 step, measured with CUDA events
+ * around individual launches (no graph): ms[0..3] = stages 0..3, averaged over
+ * `reps` steps of size dt. Advances the state by `reps` steps. */
+int vt_profile_rk4_stages(vt_ctx* ctx, double dt, int reps, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VORTEX_B200_H */

@@ -74,11 +74,38 @@ def run_case(name: str, args: list[str]) -> str:
     return out
 
 
+def quadrature_tables() -> str:
+    """Line and area rules the reference selects for integration_order 0..19
+    (Quadraturerule.cpp:125-126, :590-591), plus M^-1_ref and S_ref for p=0..3."""
+    arrays = {}
+    for io in range(20):
+        for p in range(4):
+            tmp = tempfile.mkdtemp(prefix="vt_quad_")
+            subprocess.run([HARNESS, "--nx", "2", "--ny", "2", "--p", str(p), "--io", str(io),
+                            "--steps", "0", "--no-ops", "--dump", tmp], check=True,
+                           stdout=subprocess.DEVNULL)
+            if p == 0:
+                arrays[f"line_{io}"] = np.fromfile(os.path.join(tmp, "line_quad.f64"))
+                arrays[f"area_{io}"] = np.fromfile(os.path.join(tmp, "area_quad.f64"))
+            arrays[f"minv_{io}_{p}"] = np.fromfile(os.path.join(tmp, "minv_ref.f64"))
+            arrays[f"stiff_{io}_{p}"] = np.fromfile(os.path.join(tmp, "stiff_ref.f64"))
+            arrays[f"phi_plus_{io}_{p}"] = np.fromfile(os.path.join(tmp, "phi_plus.f64"))
+            arrays[f"phi_minus_{io}_{p}"] = np.fromfile(os.path.join(tmp, "phi_minus.f64"))
+            arrays[f"nodes_ref_{p}"] = np.fromfile(os.path.join(tmp, "nodes_ref.f64"))
+            shutil.rmtree(tmp)
+    out = os.path.join(HERE, "quadrature_tables.npz")
+    np.savez_compressed(out, **arrays)
+    return out
+
+
 def main() -> int:
     if not os.path.exists(HARNESS):
         print("build the harness first: make -C oracle ref", file=sys.stderr)
         return 1
     only = set(sys.argv[1:])
+    if not only or "quadrature_tables" in only:
+        out = quadrature_tables()
+        print(f"quadrature_tables: {os.path.getsize(out) / 1024:.1f} KiB")
     for name, args in CASES.items():
         if only and name not in only:
             continue

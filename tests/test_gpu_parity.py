@@ -1,0 +1,198 @@
+"""Parity of the sm_100a stepper with the reference (goldens) and the oracle.
+
+Tolerances (the bar set for this path):
+  * state after one step: 1e-12 relative per node and component;
+  * state after the shipped 10000-step run: 1e-9 relative per node;
+  * right-hand side: 1e-12 of the component's largest magnitude (the RHS
+    passes through zero, so a per-node relative bound is meaningless there);
+  * conservation totals: drift at round-off level.
+Error detection must report the same element and check as the reference's
+first failing flux call.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import Golden, golden, golden_paths
+
+pytestmark = pytest.mark.gpu
+
+STATE_RTOL_1STEP = 1e-12
+STATE_RTOL_LONG = 1e-9
+RHS_TOL = 1e-12
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(a - b) / np.abs(b)))
+
+
+def rhs_err(a, b):
+    scale = np.max(np.abs(b), axis=(0, 1))
+    return float(np.max(np.abs(a - b) / scale))
+
+
+def problem_for(vt, g: Golden):
+    m = g.meta
+    prm = vt.make_params(m["nx"], m["ny"], p=m["p"], integration_order=m["io"],
+                         domain_x=m["domain_x"], domain_y=m["domain_y"],
+                         perturb_grid=m["perturb_grid"], U_initialization_type=m["init_type"],
+                         stepping_method=m["stepping"], time_step=m["dt"])
+    return vt.Problem(prm)
+
+
+SHORT = [p for p in golden_paths() if "10000" not in p]
+
+
+@pytest.mark.parametrize("path", SHORT, ids=lambda p: os.path.basename(p)[:-4])
+def test_rhs_and_steps_match_reference(vt, path):
+    g = Golden(path)
+    pb = problem_for(vt, g)
+    s = vt.Solver(pb)
+    np.testing.assert_array_equal(s.download(), g["U0"])
+    if "rhs0" in g:
+        assert rhs_err(s.rhs(), g["rhs0"]) < RHS_TOL
+    dt, n = g.meta["dt"], g.meta["steps"]
+    if g.meta["stepping"] == 1:
+        vt.rk4(s, dt, n)
+    else:
+        vt.forward_euler(s, dt, n)
+    U, F = s.download(with_flux=True)
+    assert rel_err(U, g["U_final"]) < STATE_RTOL_1STEP * max(1, n)
+    assert rel_err(F[np.abs(g["F_final"]) > 1e-8], g["F_final"][np.abs(g["F_final"]) > 1e-8]) < 1e-11
+    # time advances like Element::time (one += per step)
+    assert s.time == g.meta["time"]
+
+
+def test_shipped_10000_steps(vt):
+    """Config 1: T = 10*sqrt(2), 10000 RK4 steps, compared every 2500 steps."""
+    g = golden("c1_p3_io10_rk4_10000")
+    s = vt.Solver(problem_for(vt, g))
+    worst = 0.0
+    for k in range(1, 5):
+        s.rk4(g.meta["dt"], 2500)
+        e = rel_err(s.download(), g[f"U_step{2500 * k}"])
+        worst = max(worst, e)
+        assert e < STATE_RTOL_LONG, (k, e)
+    print(f"config 1 worst relative deviation over 10000 steps: {worst:.3e}")
+
+
+@pytest.mark.parametrize("p,io,nx,ny,perturb", [(3, 10, 24, 20, 0.2), (2, 10, 17, 13, 0.1),
+                                                (1, 6, 31, 9, 0.2), (3, 6, 9, 33, 0.0)])
+def test_against_oracle_other_meshes(vt, p, io, nx, ny, perturb):
+    """Seeded meshes outside the fixtures: GPU vs the oracle on the product's own operators."""
+    import vt_oracle
+    prm = vt.make_params(nx, ny, p=p, integration_order=io, perturb_grid=perturb)
+    rng = np.random.default_rng(1234 + p * 100 + nx)
+    ic = vt.vortex(epsilon=rng.uniform(0.1, 0.5), M_infty=rng.uniform(0.3, 0.7),
+                   x0=rng.uniform(-2, 2), y0=rng.uniform(-2, 2))
+    pb = vt.Problem(prm, ic)
+    om = vt_oracle.OracleMesh(p, pb.array("vertices"), pb.array("conn"), pb.array("type"),
+                              pb.array("minv_ref"), pb.array("stiff_ref"), pb.array("phi_plus"),
+                              pb.array("phi_minus"), pb.array("line_quad"))
+    U0, F0 = pb.array("U0"), pb.array("F0")
+    s = vt.Solver(pb)
+    r_ref, err = om.rhs(U0, F0)
+    assert err.code == 0
+    assert rhs_err(s.rhs(), r_ref) < RHS_TOL
+    dt = 1e-3
+    U_ref, _, err = om.step(U0, F0, dt, 3, 1)
+    assert err.code == 0
+    s.rk4(dt, 3)
+    assert rel_err(s.download(), U_ref) < 3 * STATE_RTOL_1STEP
+
+
+def test_nonphysical_state_reported_like_reference(vt):
+    """A planted negative density: same first failing element and check as the oracle."""
+    g = golden("c1_p3_io10_rk4_1step")
+    pb = problem_for(vt, g)
+    s = vt.Solver(pb)
+    U = g["U0"].copy()
+    U[77, :, 0] = -1.0
+    U[90, 3, 0] = -0.5
+    s.upload(U)
+    _, oerr = g.oracle_mesh().rhs(U, vt.flux_from_state(U))
+    with pytest.raises(vt.NonPhysicalState) as ei:
+        s.rk4(g.meta["dt"], 1)
+    assert (ei.value.code, ei.value.element, ei.value.point, ei.value.side) == \
+        (oerr.code, oerr.element, oerr.point, oerr.side)
+    assert ei.value.step == 0 and ei.value.stage == 0
+    # the context stays usable: a good state steps again
+    s.upload(g["U0"])
+    s.rk4(g.meta["dt"], 1)
+    assert rel_err(s.download(), g["U_final"]) < STATE_RTOL_1STEP
+
+
+def test_error_in_later_step_reports_step(vt):
+    """A state that turns non-physical only after a few steps reports that step."""
+    prm = vt.make_params(8, 8, p=2, integration_order=6)
+    pb = vt.Problem(prm)
+    s = vt.Solver(pb)
+    U = pb.array("U0").copy()
+    U[40, :, 3] *= 0.7  # low energy: pressure collapses after a few large steps
+    s.upload(U)
+    with pytest.raises(vt.NonPhysicalState) as ei:
+        s.rk4(0.05, 200)
+    assert ei.value.step >= 0 and 0 <= ei.value.stage < 4
+    assert 0 <= ei.value.element < pb.K
+
+
+def test_conservation_round_off(vt):
+    prm = vt.make_params(32, 32, p=3, perturb_grid=0.2)
+    s = vt.Solver(vt.Problem(prm))
+    t0 = s.totals()
+    s.rk4(2e-3, 200)
+    t1 = s.totals()
+    drift = np.abs(t1 - t0) / np.abs(t0)
+    assert np.all(drift < 1e-13), drift
+
+
+def test_upload_download_roundtrip_and_async(vt):
+    prm = vt.make_params(12, 7, p=3, perturb_grid=0.2)
+    pb = vt.Problem(prm)
+    s = vt.Solver(pb)
+    U = np.random.default_rng(3).standard_normal((pb.K, pb.Np, 4))
+    s.upload(U)
+    np.testing.assert_array_equal(s.download(), U)
+    s.upload(pb.array("U0"))
+    s.rk4(1e-3, 5)
+    a = s.download()
+    s.upload(pb.array("U0"))
+    s.rk4_async(1e-3, 5)
+    s.synchronize()
+    np.testing.assert_array_equal(s.download(), a)
+
+
+def test_device_pointer_transfer(vt):
+    import torch
+    prm = vt.make_params(10, 10, p=2)
+    pb = vt.Problem(prm)
+    s = vt.Solver(pb)
+    dU = torch.from_numpy(pb.array("U0")).cuda()
+    out = torch.empty_like(dU)
+    s.upload_device(dU.data_ptr())
+    s.download_device(out.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(dU, out)
+
+
+def test_config2_one_step_full_size(vt):
+    """768x768 cells (1,179,648 triangles), p=3, perturb 0.2, dt 1.4e-5: one RK4
+    step against the oracle on every node, plus conservation."""
+    import vt_oracle
+    prm = vt.make_params(768, 768, p=3, integration_order=10, perturb_grid=0.2, time_step=1.4e-5)
+    pb = vt.Problem(prm)
+    s = vt.Solver(pb)
+    t0 = s.totals()
+    s.rk4(1.4e-5, 1)
+    U = s.download()
+    om = vt_oracle.OracleMesh(3, pb.array("vertices"), pb.array("conn"), pb.array("type"),
+                              pb.array("minv_ref"), pb.array("stiff_ref"), pb.array("phi_plus"),
+                              pb.array("phi_minus"), pb.array("line_quad"))
+    U_ref, _, err = om.step(pb.array("U0"), pb.array("F0"), 1.4e-5, 1, 1)
+    assert err.code == 0
+    e = rel_err(U, U_ref)
+    print(f"config 2 one-step max relative deviation: {e:.3e}")
+    assert e < STATE_RTOL_1STEP
+    drift = np.abs(s.totals() - t0) / np.abs(t0)
+    assert np.all(drift < 1e-13), drift

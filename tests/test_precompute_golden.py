@@ -1,0 +1,125 @@
+"""The product's host precompute against the reference's own outputs.
+
+Mesh, connectivity, quadrature, reference operators, per-element geometry,
+face tables and the initial condition must equal the reference's bit for bit
+(tests/golden/*.npz, written by the reference compiled from its sources).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, Golden, golden_paths
+
+CASES = golden_paths()
+ARRAYS = ["vertices", "conn", "type", "nodes_ref", "line_quad", "area_quad", "minv_ref",
+          "stiff_ref", "phi_plus", "phi_minus", "jac", "jinv", "detj", "detjinv", "normals",
+          "sides", "nodes_phys", "U0", "F0"]
+
+
+def problem_for(vt, g: Golden):
+    m = g.meta
+    prm = vt.make_params(m["nx"], m["ny"], p=m["p"], integration_order=m["io"],
+                         domain_x=m["domain_x"], domain_y=m["domain_y"],
+                         perturb_grid=m["perturb_grid"], U_initialization_type=m["init_type"],
+                         stepping_method=m["stepping"], time_step=m["dt"])
+    return vt.Problem(prm)
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: os.path.basename(p)[:-4])
+def test_precompute_matches_reference_bitwise(vt, path):
+    g = Golden(path)
+    pb = problem_for(vt, g)
+    assert (pb.K, pb.Np, pb.nfq) == (g.K, g.Np, g.nfq)
+    for name in ARRAYS:
+        np.testing.assert_array_equal(pb.array(name), g[name], err_msg=name)
+
+
+def test_quadrature_and_reference_operators_all_orders(vt):
+    z = np.load(os.path.join(GOLDEN_DIR, "quadrature_tables.npz"))
+    for io in range(20):
+        for p in range(4):
+            if not np.all(np.isfinite(z[f"minv_{io}_{p}"])):
+                # a 1-point area rule makes the p >= 1 mass matrix singular; the
+                # reference carries inf/nan operators, the product refuses
+                with pytest.raises(vt.VortexError) as ei:
+                    vt.Problem(vt.make_params(2, 2, p=p, integration_order=io))
+                assert ei.value.status == vt.VT_ERR_UNSUPPORTED
+                continue
+            pb = vt.Problem(vt.make_params(2, 2, p=p, integration_order=io))
+            np.testing.assert_array_equal(pb.array("line_quad").ravel(), z[f"line_{io}"])
+            np.testing.assert_array_equal(pb.array("nodes_ref").ravel(), z[f"nodes_ref_{p}"])
+            np.testing.assert_array_equal(pb.array("phi_plus").ravel(), z[f"phi_plus_{io}_{p}"])
+            np.testing.assert_array_equal(pb.array("phi_minus").ravel(), z[f"phi_minus_{io}_{p}"])
+            if io <= 10:
+                np.testing.assert_array_equal(pb.array("area_quad").ravel(), z[f"area_{io}"])
+                np.testing.assert_array_equal(pb.array("minv_ref").ravel(), z[f"minv_{io}_{p}"])
+                np.testing.assert_array_equal(pb.array("stiff_ref").ravel(), z[f"stiff_{io}_{p}"])
+            else:
+                # orders 11-19 use the degree-10 rule, exact for these integrands
+                np.testing.assert_allclose(pb.array("minv_ref").ravel(), z[f"minv_{io}_{p}"],
+                                           rtol=1e-12, atol=1e-12)
+                np.testing.assert_allclose(pb.array("stiff_ref").ravel(), z[f"stiff_{io}_{p}"],
+                                           rtol=1e-12, atol=1e-13)
+
+
+INPUT_TEXT = """// a comment line without the separator is ignored
+p=3
+domain_x=10.0 //cm
+domain_y=10.0 //cm
+num_element_in_x=8
+num_element_in_y=8
+perturb_grid=0.2
+integration_order=10
+simulation_time=14.14213562373
+number_time_steps=10000
+write_every_steps=250
+U_initialization_type=0
+stepping_method=1
+"""
+
+
+def test_input_file_keys_and_quirks(vt, tmp_path):
+    path = tmp_path / "input"
+    path.write_text(INPUT_TEXT)
+    prm = vt.read_input_files(str(path))
+    assert prm.p == 3 and prm.num_element_in_x == 8 and prm.num_element_in_y == 8
+    assert prm.domain_x == np.float32(10.0) and prm.domain_y == np.float32(10.0)
+    # std::stoi on "0.2" (Parameters.cpp:55): the perturbation is silently 0
+    assert prm.perturb_grid == 0.0
+    assert prm.simulation_time == np.float32(14.14213562373)
+    # time step from the strings in double (Parameters.cpp:59)
+    assert prm.time_step == float("14.14213562373") / float("10000")
+    assert prm.integration_order == 10 and prm.write_every_steps == 250
+    assert prm.U_initialization_type == 0 and prm.stepping_method == 1
+    # last definition wins, like the reference's map
+    prm2 = vt.parse_input(INPUT_TEXT + "p=2\n")
+    assert prm2.p == 2
+
+
+def test_input_file_errors(vt, tmp_path):
+    with pytest.raises(vt.VortexError) as ei:
+        vt.parse_input(INPUT_TEXT.replace("num_element_in_y=8\n", ""))
+    assert ei.value.status == vt.VT_ERR_INVALID
+    assert "num_element_in_y" in str(ei.value)
+    with pytest.raises(vt.VortexError):
+        vt.read_input_files(str(tmp_path / "does_not_exist"))
+    with pytest.raises(vt.VortexError) as ei:
+        vt.Problem(vt.make_params(4, 4, p=4))
+    assert ei.value.status == vt.VT_ERR_UNSUPPORTED
+
+
+def test_flux_from_state_matches_reference(vt):
+    g = Golden(os.path.join(GOLDEN_DIR, "p3_io10_16x16_pert_rk4.npz"))
+    np.testing.assert_array_equal(vt.flux_from_state(g["U_final"]), g["F_final"])
+
+
+def test_parameterised_vortex_reduces_to_reference(vt):
+    """vortex() with the reference's numbers reproduces the hard-coded IC."""
+    prm = vt.make_params(8, 8)
+    a = vt.Problem(prm).array("U0")
+    b = vt.Problem(prm, vt.vortex(epsilon=0.3, x0=0.0, y0=0.0)).array("U0")
+    np.testing.assert_array_equal(a, b)
+    c = vt.Problem(prm, vt.vortex(epsilon=0.35, M_infty=0.4, x0=0.4, y0=-0.25)).array("U0")
+    assert not np.array_equal(a, c)
+    assert np.all(c[..., 0] > 0)

@@ -1,0 +1,603 @@
+// C ABI of the device solver (include/vortex_b200.h, "drop-in boundary").
+//
+// vt_create folds the reference-space operators into the per-stage kernel
+// parameter block and uploads packed per-element geometry; vt_step_rk4 replays
+// a captured CUDA graph of the four fused stage kernels once per step.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vortex_b200.h"
+#include "vt_common.h"
+#include "vt_precompute.h"
+#include "vt_stage.cuh"
+
+namespace vt {
+namespace {
+
+constexpr int kThreads = 128;
+
+using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, int, cudaStream_t);
+
+template <int P, int NFQ>
+cudaError_t launch_stage(const StageArgs& a, const double* ops, int grid, cudaStream_t st) {
+  StageOps<P, NFQ> o;
+  static_assert(sizeof(StageOps<P, NFQ>) % sizeof(double) == 0, "operator block is doubles");
+  std::memcpy(&o, ops, sizeof(o));
+  stage_kernel<P, NFQ><<<grid, kThreads, 0, st>>>(a, o);
+  return cudaGetLastError();
+}
+
+template <int P>
+LaunchFn launcher_for_nfq(int nfq) {
+  switch (nfq) {
+    case 1: return launch_stage<P, 1>;
+    case 2: return launch_stage<P, 2>;
+    case 3: return launch_stage<P, 3>;
+    case 4: return launch_stage<P, 4>;
+    case 5: return launch_stage<P, 5>;
+    case 6: return launch_stage<P, 6>;
+    case 7: return launch_stage<P, 7>;
+    case 8: return launch_stage<P, 8>;
+    case 9: return launch_stage<P, 9>;
+    case 10: return launch_stage<P, 10>;
+    default: return nullptr;
+  }
+}
+
+LaunchFn select_launcher(int p, int nfq) {
+  switch (p) {
+    case 0: return launcher_for_nfq<0>(nfq);
+    case 1: return launcher_for_nfq<1>(nfq);
+    case 2: return launcher_for_nfq<2>(nfq);
+    case 3: return launcher_for_nfq<3>(nfq);
+    default: return nullptr;
+  }
+}
+
+// Folds M_ref^-1 into the volume and lift operators and restricts the face
+// tables to each side's nodes, in the layout of StageOps<P, NFQ>.
+std::vector<double> fold_operators(int p, int nfq, const double* minv, const double* stiff,
+                                   const double* line, const double* phi_plus,
+                                   const double* phi_minus) {
+  const int Np = np_of(p), NE = p + 1;
+  std::vector<double> ops;
+  ops.reserve(2 * Np * Np + 3 * Np * nfq + 6 * nfq * NE);
+  for (int d = 0; d < 2; ++d)
+    for (int i = 0; i < Np; ++i)
+      for (int j = 0; j < Np; ++j) {
+        long double s = 0;
+        for (int k = 0; k < Np; ++k)
+          s += static_cast<long double>(minv[i * Np + k]) * stiff[(d * Np + k) * Np + j];
+        ops.push_back(static_cast<double>(s));
+      }
+  for (int sd = 0; sd < 3; ++sd)
+    for (int i = 0; i < Np; ++i)
+      for (int q = 0; q < nfq; ++q) {
+        long double s = 0;
+        for (int j = 0; j < Np; ++j)
+          s += static_cast<long double>(minv[i * Np + j]) * phi_plus[(sd * Np + j) * nfq + q];
+        ops.push_back(static_cast<double>(s * line[2 * q + 1]));
+      }
+  for (int sd = 0; sd < 3; ++sd)
+    for (int q = 0; q < nfq; ++q)
+      for (int k = 0; k < NE; ++k) ops.push_back(phi_plus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
+  for (int sd = 0; sd < 3; ++sd)
+    for (int q = 0; q < nfq; ++q)
+      for (int k = 0; k < NE; ++k) ops.push_back(phi_minus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
+  return ops;
+}
+
+// Host AoS (K x Np x 4) <-> device SoA-of-double2 rows, through a shared
+// memory tile of 32 elements so both sides stay coalesced.
+constexpr int kTileE = 32;
+
+__global__ void aos_to_soa_kernel(const double2* __restrict__ aos, double2* __restrict__ soa, int K,
+                                  int Np, long long Kpad) {
+  extern __shared__ double2 tile[];
+  const int R = 2 * Np;
+  const int e0 = blockIdx.x * kTileE;
+  const int ne = min(kTileE, K - e0);
+  for (int l = threadIdx.x; l < ne * R; l += blockDim.x) tile[l] = aos[static_cast<long long>(e0) * R + l];
+  __syncthreads();
+  for (int l = threadIdx.x; l < kTileE * R; l += blockDim.x) {
+    const int r = l / kTileE, j = l % kTileE;
+    if (j < ne) soa[r * Kpad + e0 + j] = tile[j * R + r];
+  }
+}
+
+__global__ void soa_to_aos_kernel(const double2* __restrict__ soa, double2* __restrict__ aos, int K,
+                                  int Np, long long Kpad) {
+  extern __shared__ double2 tile[];
+  const int R = 2 * Np;
+  const int e0 = blockIdx.x * kTileE;
+  const int ne = min(kTileE, K - e0);
+  for (int l = threadIdx.x; l < kTileE * R; l += blockDim.x) {
+    const int r = l / kTileE, j = l % kTileE;
+    if (j < ne) tile[j * R + r] = soa[r * Kpad + e0 + j];
+  }
+  __syncthreads();
+  for (int l = threadIdx.x; l < ne * R; l += blockDim.x) aos[static_cast<long long>(e0) * R + l] = tile[l];
+}
+
+// Conservation totals: per block, sum over its elements of detJ * W . U in a
+// fixed order; a second single-block pass sums the partials in a fixed order.
+__global__ void totals_partial_kernel(const double2* __restrict__ U, const double2* __restrict__ geo,
+                                      const double* __restrict__ W, int K, int Np, long long Kpad,
+                                      double* __restrict__ partial) {
+  __shared__ double red[4][256];
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[4] = {0, 0, 0, 0};
+  if (e < K) {
+    const double detj = geo[6 * Kpad + e].y;
+    for (int i = 0; i < Np; ++i) {
+      const double2 a = U[(2 * i) * Kpad + e], b = U[(2 * i + 1) * Kpad + e];
+      acc[0] += W[i] * a.x;
+      acc[1] += W[i] * a.y;
+      acc[2] += W[i] * b.x;
+      acc[3] += W[i] * b.y;
+    }
+    for (int c = 0; c < 4; ++c) acc[c] *= detj;
+  }
+  for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) partial[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void totals_final_kernel(const double* __restrict__ partial, int nblocks,
+                                    double* __restrict__ out) {
+  __shared__ double red[4][256];
+  double acc[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int c = 0; c < 4; ++c) acc[c] += partial[b * 4 + c];
+  for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+std::string cuda_msg(const char* what, cudaError_t e) {
+  return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+}  // namespace
+}  // namespace vt
+
+struct vt_ctx {
+  std::mutex mu;
+  int device = 0, p = 0, Np = 0, nfq = 0, K = 0;
+  long long Kpad = 0;
+  int grid = 0;
+  cudaStream_t stream = nullptr;
+  double2 *U = nullptr, *A = nullptr, *Sa = nullptr, *Sb = nullptr, *R = nullptr;
+  double2* geo = nullptr;
+  int4* nbr = nullptr;
+  unsigned long long* err = nullptr;
+  double2* aos = nullptr;
+  double *W = nullptr, *partial = nullptr, *tot = nullptr;
+  std::vector<double> ops;
+  vt::LaunchFn launch = nullptr;
+  double time = 0.0;
+  cudaGraphExec_t rk4_graph = nullptr;
+  double rk4_graph_dt = 0.0;
+  vt_error_info last{};
+  int pending_steps = 0;
+  double pending_dt = 0.0;
+};
+
+namespace {
+
+using vt::fail;
+
+template <typename T>
+cudaError_t alloc(T** p, size_t bytes) {
+  return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
+void release(vt_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->rk4_graph) cudaGraphExecDestroy(c->rk4_graph);
+  void* bufs[] = {c->U, c->A, c->Sa, c->Sb, c->R, c->geo, c->nbr, c->err, c->aos, c->W, c->partial, c->tot};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, double2* acc, double2* out,
+                         int stage, double c_acc, double c_out) {
+  vt::StageArgs a;
+  a.in = in;
+  a.base = base;
+  a.acc = acc;
+  a.out = out;
+  a.geo = c->geo;
+  a.nbr = c->nbr;
+  a.err = c->err;
+  a.Kpad = c->Kpad;
+  a.K = c->K;
+  a.stage = stage;
+  a.c_acc = c_acc;
+  a.c_out = c_out;
+  return a;
+}
+
+cudaError_t enqueue_rk4_step(vt_ctx* c, double dt) {
+  cudaError_t e;
+  const double* ops = c->ops.data();
+  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2), ops, c->grid, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2), ops, c->grid, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt), ops, c->grid, c->stream))) return e;
+  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6), ops, c->grid, c->stream);
+}
+
+cudaError_t reset_error_words(vt_ctx* c) {
+  cudaError_t e = cudaMemsetAsync(c->err, 0xFF, sizeof(unsigned long long), c->stream);
+  if (e) return e;
+  return cudaMemsetAsync(c->err + 1, 0, 3 * sizeof(unsigned long long), c->stream);
+}
+
+// Waits for the stream, decodes the first-error key and advances the clock.
+int finish(vt_ctx* c, int nsteps, double dt) {
+  unsigned long long key = ~0ull;
+  cudaError_t e = cudaMemcpyAsync(&key, c->err, sizeof(key), cudaMemcpyDeviceToHost, c->stream);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("step", e));
+  for (int s = 0; s < nsteps; ++s) c->time += dt;  // Element::time += t_step per step
+  c->last = vt_error_info{};
+  if (key == ~0ull) return VT_OK;
+  const unsigned long long epoch = key >> 40;
+  unsigned long long local = key & ((1ull << 40) - 1);
+  c->last.code = static_cast<int>(local & 3ull);
+  local >>= 2;
+  c->last.side = static_cast<int>(local % 3ull);
+  local /= 3ull;
+  c->last.point = static_cast<int>(local % static_cast<unsigned long long>(c->nfq));
+  c->last.element = static_cast<int>(local / static_cast<unsigned long long>(c->nfq));
+  c->last.step = static_cast<int64_t>(epoch / 4);
+  c->last.stage = static_cast<int>(epoch % 4);
+  return fail(c->last.code, "Non-physical state (code " + std::to_string(c->last.code) + ") at element " +
+                                std::to_string(c->last.element) + ", step " + std::to_string(c->last.step) +
+                                ", stage " + std::to_string(c->last.stage));
+}
+
+int ensure_aos(vt_ctx* c) {
+  if (c->aos) return VT_OK;
+  cudaError_t e = alloc(&c->aos, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np);
+  return e ? fail(VT_ERR_NO_MEMORY, vt::cuda_msg("staging buffer", e)) : VT_OK;
+}
+
+cudaError_t aos_to_soa(vt_ctx* c, const double* src, double2* dst) {
+  const int blocks = (c->K + vt::kTileE - 1) / vt::kTileE;
+  const size_t smem = sizeof(double2) * vt::kTileE * 2 * c->Np;
+  vt::aos_to_soa_kernel<<<blocks, 256, smem, c->stream>>>(reinterpret_cast<const double2*>(src), dst, c->K,
+                                                          c->Np, c->Kpad);
+  return cudaGetLastError();
+}
+
+cudaError_t soa_to_aos(vt_ctx* c, const double2* src, double* dst) {
+  const int blocks = (c->K + vt::kTileE - 1) / vt::kTileE;
+  const size_t smem = sizeof(double2) * vt::kTileE * 2 * c->Np;
+  vt::soa_to_aos_kernel<<<blocks, 256, smem, c->stream>>>(src, reinterpret_cast<double2*>(dst), c->K, c->Np,
+                                                          c->Kpad);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
+  auto set = [&](int s) {
+    if (status) *status = s;
+  };
+  if (!d || !d->element_type || !d->neighbours || !d->det_jacobian || !d->inv_jacobian || !d->normals ||
+      !d->side_lengths || !d->inv_mass_ref || !d->stiffness_ref || !d->line_quadrature || !d->phi_plus ||
+      !d->phi_minus) {
+    set(fail(VT_ERR_INVALID, "vt_create: null descriptor field"));
+    return nullptr;
+  }
+  if (d->p < 0 || d->p > 3) {
+    set(fail(VT_ERR_UNSUPPORTED, "vt_create: p must be 0..3"));
+    return nullptr;
+  }
+  if (d->n_line_points < 1 || d->n_line_points > 10) {
+    set(fail(VT_ERR_UNSUPPORTED, "vt_create: n_line_points must be 1..10"));
+    return nullptr;
+  }
+  if (d->n_elements < 1) {
+    set(fail(VT_ERR_INVALID, "vt_create: n_elements must be positive"));
+    return nullptr;
+  }
+  const int K = d->n_elements;
+  for (int n = 0; n < 3 * K; ++n)
+    if (d->neighbours[n] < 0 || d->neighbours[n] >= K) {
+      set(fail(VT_ERR_INVALID, "vt_create: neighbour index out of range at element " + std::to_string(n / 3)));
+      return nullptr;
+    }
+  cudaError_t e = cudaSetDevice(device);
+  if (e) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("cudaSetDevice", e)));
+    return nullptr;
+  }
+  auto* c = new vt_ctx();
+  c->device = device;
+  c->p = d->p;
+  c->Np = vt::np_of(d->p);
+  c->nfq = d->n_line_points;
+  c->K = K;
+  c->Kpad = (static_cast<long long>(K) + 127) / 128 * 128;
+  c->grid = (K + vt::kThreads - 1) / vt::kThreads;
+  c->launch = vt::select_launcher(c->p, c->nfq);
+  c->ops = vt::fold_operators(c->p, c->nfq, d->inv_mass_ref, d->stiffness_ref, d->line_quadrature,
+                              d->phi_plus, d->phi_minus);
+
+  // packed geometry and side-ordered neighbours (Evolve.cpp:167-202)
+  const long long KP = c->Kpad;
+  std::vector<double2> geo(7 * static_cast<size_t>(KP), make_double2(0.0, 0.0));
+  std::vector<int4> nbr(static_cast<size_t>(KP), make_int4(0, 0, 0, 0));
+  for (int n = 0; n < K; ++n) {
+    const double* ji = d->inv_jacobian + 4 * static_cast<size_t>(n);
+    const double* nv = d->normals + 6 * static_cast<size_t>(n);
+    const double* ln = d->side_lengths + 3 * static_cast<size_t>(n);
+    const double det = d->det_jacobian[n];
+    geo[0 * KP + n] = make_double2(ji[0], ji[1]);
+    geo[1 * KP + n] = make_double2(ji[2], ji[3]);
+    for (int s = 0; s < 3; ++s) geo[(2 + s) * KP + n] = make_double2(nv[2 * s], nv[2 * s + 1]);
+    geo[5 * KP + n] = make_double2(ln[0] / det, ln[1] / det);
+    geo[6 * KP + n] = make_double2(ln[2] / det, det);
+    const int right = d->neighbours[3 * n], left = d->neighbours[3 * n + 1], vert = d->neighbours[3 * n + 2];
+    nbr[n] = d->element_type[n] == 0 ? make_int4(vert, right, left, 0) : make_int4(vert, left, right, 0);
+  }
+  // W_i = integral of phi_i = sum_j M_ref[i][j] (the basis sums to one)
+  std::vector<double> m(d->inv_mass_ref, d->inv_mass_ref + c->Np * c->Np), W(c->Np, 0.0);
+  vt::invert_gauss_jordan(c->Np, &m);
+  for (int i = 0; i < c->Np; ++i)
+    for (int j = 0; j < c->Np; ++j) W[i] += m[i * c->Np + j];
+
+  const size_t state_bytes = sizeof(double2) * 2 * c->Np * static_cast<size_t>(KP);
+  const int tot_blocks = (K + 255) / 256;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) || (e = alloc(&c->U, state_bytes)) ||
+      (e = alloc(&c->A, state_bytes)) || (e = alloc(&c->Sa, state_bytes)) || (e = alloc(&c->Sb, state_bytes)) ||
+      (e = alloc(&c->geo, geo.size() * sizeof(double2))) || (e = alloc(&c->nbr, nbr.size() * sizeof(int4))) ||
+      (e = alloc(&c->err, 4 * sizeof(unsigned long long))) || (e = alloc(&c->W, sizeof(double) * c->Np)) ||
+      (e = alloc(&c->partial, sizeof(double) * 4 * tot_blocks)) || (e = alloc(&c->tot, sizeof(double) * 4))) {
+    const bool oom = e == cudaErrorMemoryAllocation;
+    set(fail(oom ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, vt::cuda_msg("vt_create", e)));
+    release(c);
+    return nullptr;
+  }
+  if ((e = cudaMemcpy(c->geo, geo.data(), geo.size() * sizeof(double2), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->nbr, nbr.data(), nbr.size() * sizeof(int4), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->W, W.data(), sizeof(double) * c->Np, cudaMemcpyHostToDevice)) ||
+      (e = cudaMemset(c->U, 0, state_bytes)) || (e = cudaMemset(c->A, 0, state_bytes)) ||
+      (e = cudaMemset(c->Sa, 0, state_bytes)) || (e = cudaMemset(c->Sb, 0, state_bytes))) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_create upload", e)));
+    release(c);
+    return nullptr;
+  }
+  set(VT_OK);
+  return c;
+}
+
+void vt_destroy(vt_ctx* c) { release(c); }
+
+int vt_upload_state_device(vt_ctx* c, const double* dU) {
+  if (!c || !dU) return fail(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaError_t e = aos_to_soa(c, dU, c->U);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("upload", e)) : VT_OK;
+}
+
+int vt_upload_state(vt_ctx* c, const double* U) {
+  if (!c || !U) return fail(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  int st = ensure_aos(c);
+  if (st) return st;
+  cudaError_t e = cudaMemcpyAsync(c->aos, U, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np,
+                                  cudaMemcpyHostToDevice, c->stream);
+  if (!e) e = aos_to_soa(c, reinterpret_cast<const double*>(c->aos), c->U);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("upload", e)) : VT_OK;
+}
+
+int vt_download_state_device(vt_ctx* c, double* dU) {
+  if (!c || !dU) return fail(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaError_t e = soa_to_aos(c, c->U, dU);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("download", e)) : VT_OK;
+}
+
+int vt_download_state(vt_ctx* c, double* U, double* F) {
+  if (!c || !U) return fail(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  int st = ensure_aos(c);
+  if (st) return st;
+  cudaError_t e = soa_to_aos(c, c->U, reinterpret_cast<double*>(c->aos));
+  if (!e)
+    e = cudaMemcpyAsync(U, c->aos, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np,
+                        cudaMemcpyDeviceToHost, c->stream);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("download", e));
+  if (F) vt::flux_from_state(c->K, c->Np, U, F);
+  return VT_OK;
+}
+
+static int rk4_enqueue(vt_ctx* c, double dt, int nsteps) {
+  cudaError_t e = reset_error_words(c);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("reset", e));
+  if (!c->rk4_graph || c->rk4_graph_dt != dt) {
+    if (c->rk4_graph) {
+      cudaGraphExecDestroy(c->rk4_graph);
+      c->rk4_graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (!e) {
+      const cudaError_t le = enqueue_rk4_step(c, dt);
+      e = cudaStreamEndCapture(c->stream, &g);
+      if (le) e = le;
+    }
+    if (!e) e = cudaGraphInstantiate(&c->rk4_graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("graph capture", e));
+    c->rk4_graph_dt = dt;
+  }
+  for (int s = 0; s < nsteps; ++s)
+    if ((e = cudaGraphLaunch(c->rk4_graph, c->stream))) return fail(VT_ERR_CUDA, vt::cuda_msg("graph launch", e));
+  c->pending_steps += nsteps;
+  c->pending_dt = dt;
+  return VT_OK;
+}
+
+int vt_step_rk4_async(vt_ctx* c, double dt, int nsteps) {
+  if (!c || nsteps < 0) return fail(VT_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
+  return rk4_enqueue(c, dt, nsteps);
+}
+
+int vt_synchronize(vt_ctx* c) {
+  if (!c) return fail(VT_ERR_INVALID, "null context");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const int n = c->pending_steps;
+  c->pending_steps = 0;
+  return finish(c, n, c->pending_dt);
+}
+
+int vt_step_rk4(vt_ctx* c, double dt, int nsteps) {
+  if (!c || nsteps < 0) return fail(VT_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
+  int st = rk4_enqueue(c, dt, nsteps);
+  if (st) return st;
+  c->pending_steps = 0;
+  return finish(c, nsteps, dt);
+}
+
+int vt_step_euler(vt_ctx* c, double dt, int nsteps) {
+  if (!c || nsteps < 0) return fail(VT_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
+  cudaError_t e = reset_error_words(c);
+  for (int s = 0; s < nsteps && !e; ++s) {
+    // double buffer: the neighbours of an element read the old state
+    e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, vt::kStageEuler, 0.0, dt), c->ops.data(), c->grid,
+                  c->stream);
+    std::swap(c->U, c->Sa);
+  }
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("euler", e));
+  // the RK4 graph captured the old buffer roles
+  if (nsteps % 2 && c->rk4_graph) {
+    cudaGraphExecDestroy(c->rk4_graph);
+    c->rk4_graph = nullptr;
+  }
+  return finish(c, nsteps, dt);
+}
+
+int vt_rhs(vt_ctx* c, double* Udot) {
+  if (!c || !Udot) return fail(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  int st = ensure_aos(c);
+  if (st) return st;
+  cudaError_t e = cudaSuccess;
+  if (!c->R) e = alloc(&c->R, sizeof(double2) * 2 * c->Np * static_cast<size_t>(c->Kpad));
+  if (!e) e = reset_error_words(c);
+  if (!e)
+    e = c->launch(stage_args(c, c->U, c->U, c->A, c->R, vt::kStageRhs, 0.0, 0.0), c->ops.data(), c->grid,
+                  c->stream);
+  if (!e) e = soa_to_aos(c, c->R, reinterpret_cast<double*>(c->aos));
+  if (!e)
+    e = cudaMemcpyAsync(Udot, c->aos, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np,
+                        cudaMemcpyDeviceToHost, c->stream);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("rhs", e));
+  return finish(c, 0, 0.0);
+}
+
+int vt_last_error(const vt_ctx* c, vt_error_info* out) {
+  if (!c || !out) return fail(VT_ERR_INVALID, "null argument");
+  *out = c->last;
+  return VT_OK;
+}
+
+double vt_get_time(const vt_ctx* c) { return c ? c->time : 0.0; }
+
+int vt_set_time(vt_ctx* c, double t) {
+  if (!c) return fail(VT_ERR_INVALID, "null context");
+  c->time = t;
+  return VT_OK;
+}
+
+int vt_totals(vt_ctx* c, double* out) {
+  if (!c || !out) return fail(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const int blocks = (c->K + 255) / 256;
+  vt::totals_partial_kernel<<<blocks, 256, 0, c->stream>>>(c->U, c->geo, c->W, c->K, c->Np, c->Kpad, c->partial);
+  vt::totals_final_kernel<<<1, 256, 0, c->stream>>>(c->partial, blocks, c->tot);
+  cudaError_t e = cudaGetLastError();
+  if (!e) e = cudaMemcpyAsync(out, c->tot, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("totals", e)) : VT_OK;
+}
+
+void* vt_stream(vt_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int vt_profile_rk4_stages(vt_ctx* c, double dt, int reps, float* ms) {
+  if (!c || !ms || reps < 1) return fail(VT_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaEvent_t ev[5];
+  for (auto& x : ev) cudaEventCreate(&x);
+  double acc[4] = {0, 0, 0, 0};
+  cudaError_t e = reset_error_words(c);
+  const double* ops = c->ops.data();
+  for (int r = 0; r < reps && !e; ++r) {
+    const vt::StageArgs args[4] = {stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2),
+                                   stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2),
+                                   stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt),
+                                   stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6)};
+    cudaEventRecord(ev[0], c->stream);
+    for (int s = 0; s < 4 && !e; ++s) {
+      e = c->launch(args[s], ops, c->grid, c->stream);
+      cudaEventRecord(ev[s + 1], c->stream);
+    }
+    if (!e) e = cudaEventSynchronize(ev[4]);
+    for (int s = 0; s < 4 && !e; ++s) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[s], ev[s + 1]);
+      acc[s] += t;
+    }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("profile", e));
+  for (int s = 0; s < 4; ++s) ms[s] = static_cast<float>(acc[s] / reps);
+  return finish(c, reps, dt);
+}
+
+}  // extern "C"
