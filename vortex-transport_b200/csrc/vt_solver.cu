@@ -14,48 +14,72 @@
 #include "../../include/vortex_b200.h"
 #include "vt_common.h"
 #include "vt_precompute.h"
-#include "vt_stage.cuh"
+#include "vt_tile.cuh"
 
 namespace vt {
 namespace {
 
-constexpr int kThreads = 128;
+// Elements per block of the tiled stage kernel (4 threads per element).
+constexpr int kTileElems = 64;
 
-using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, int, cudaStream_t);
+using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, cudaStream_t);
+
+// Opts the instantiation into its dynamic shared memory size; called by
+// vt_create on the context's device, before any launch or graph capture.
+template <int P, int NFQ>
+cudaError_t configure_stage() {
+  using Lay = TileLayout<P, NFQ, kTileElems>;
+  return cudaFuncSetAttribute(tile_stage_kernel<P, NFQ, kTileElems>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
+}
 
 template <int P, int NFQ>
-cudaError_t launch_stage(const StageArgs& a, const double* ops, int grid, cudaStream_t st) {
+cudaError_t launch_stage(const StageArgs& a, const double* ops, cudaStream_t st) {
+  using Lay = TileLayout<P, NFQ, kTileElems>;
   StageOps<P, NFQ> o;
   static_assert(sizeof(StageOps<P, NFQ>) % sizeof(double) == 0, "operator block is doubles");
   std::memcpy(&o, ops, sizeof(o));
-  stage_kernel<P, NFQ><<<grid, kThreads, 0, st>>>(a, o);
+  const int grid = (a.K + kTileElems - 1) / kTileElems;
+  tile_stage_kernel<P, NFQ, kTileElems><<<grid, 4 * kTileElems, Lay::kBytes, st>>>(a, o);
   return cudaGetLastError();
 }
 
+using ConfigFn = cudaError_t (*)();
+
+struct StageKernel {
+  LaunchFn launch = nullptr;
+  ConfigFn configure = nullptr;
+};
+
+template <int P, int NFQ>
+StageKernel stage_kernel_of() {
+  return StageKernel{launch_stage<P, NFQ>, configure_stage<P, NFQ>};
+}
+
 template <int P>
-LaunchFn launcher_for_nfq(int nfq) {
+StageKernel kernel_for_nfq(int nfq) {
   switch (nfq) {
-    case 1: return launch_stage<P, 1>;
-    case 2: return launch_stage<P, 2>;
-    case 3: return launch_stage<P, 3>;
-    case 4: return launch_stage<P, 4>;
-    case 5: return launch_stage<P, 5>;
-    case 6: return launch_stage<P, 6>;
-    case 7: return launch_stage<P, 7>;
-    case 8: return launch_stage<P, 8>;
-    case 9: return launch_stage<P, 9>;
-    case 10: return launch_stage<P, 10>;
-    default: return nullptr;
+    case 1: return stage_kernel_of<P, 1>();
+    case 2: return stage_kernel_of<P, 2>();
+    case 3: return stage_kernel_of<P, 3>();
+    case 4: return stage_kernel_of<P, 4>();
+    case 5: return stage_kernel_of<P, 5>();
+    case 6: return stage_kernel_of<P, 6>();
+    case 7: return stage_kernel_of<P, 7>();
+    case 8: return stage_kernel_of<P, 8>();
+    case 9: return stage_kernel_of<P, 9>();
+    case 10: return stage_kernel_of<P, 10>();
+    default: return StageKernel{};
   }
 }
 
-LaunchFn select_launcher(int p, int nfq) {
+StageKernel select_kernel(int p, int nfq) {
   switch (p) {
-    case 0: return launcher_for_nfq<0>(nfq);
-    case 1: return launcher_for_nfq<1>(nfq);
-    case 2: return launcher_for_nfq<2>(nfq);
-    case 3: return launcher_for_nfq<3>(nfq);
-    default: return nullptr;
+    case 0: return kernel_for_nfq<0>(nfq);
+    case 1: return kernel_for_nfq<1>(nfq);
+    case 2: return kernel_for_nfq<2>(nfq);
+    case 3: return kernel_for_nfq<3>(nfq);
+    default: return StageKernel{};
   }
 }
 
@@ -180,7 +204,6 @@ struct vt_ctx {
   std::mutex mu;
   int device = 0, p = 0, Np = 0, nfq = 0, K = 0;
   long long Kpad = 0;
-  int grid = 0;
   cudaStream_t stream = nullptr;
   double2 *U = nullptr, *A = nullptr, *Sa = nullptr, *Sb = nullptr, *R = nullptr;
   double2* geo = nullptr;
@@ -239,10 +262,10 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
 cudaError_t enqueue_rk4_step(vt_ctx* c, double dt) {
   cudaError_t e;
   const double* ops = c->ops.data();
-  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2), ops, c->grid, c->stream))) return e;
-  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2), ops, c->grid, c->stream))) return e;
-  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt), ops, c->grid, c->stream))) return e;
-  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6), ops, c->grid, c->stream);
+  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2), ops, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2), ops, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt), ops, c->stream))) return e;
+  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6), ops, c->stream);
 }
 
 cudaError_t reset_error_words(vt_ctx* c) {
@@ -341,8 +364,13 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
   c->nfq = d->n_line_points;
   c->K = K;
   c->Kpad = (static_cast<long long>(K) + 127) / 128 * 128;
-  c->grid = (K + vt::kThreads - 1) / vt::kThreads;
-  c->launch = vt::select_launcher(c->p, c->nfq);
+  const vt::StageKernel sk = vt::select_kernel(c->p, c->nfq);
+  c->launch = sk.launch;
+  if ((e = sk.configure())) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
+    delete c;
+    return nullptr;
+  }
   c->ops = vt::fold_operators(c->p, c->nfq, d->inv_mass_ref, d->stiffness_ref, d->line_quadrature,
                               d->phi_plus, d->phi_minus);
 
@@ -506,7 +534,7 @@ int vt_step_euler(vt_ctx* c, double dt, int nsteps) {
   cudaError_t e = reset_error_words(c);
   for (int s = 0; s < nsteps && !e; ++s) {
     // double buffer: the neighbours of an element read the old state
-    e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, vt::kStageEuler, 0.0, dt), c->ops.data(), c->grid,
+    e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, vt::kStageEuler, 0.0, dt), c->ops.data(),
                   c->stream);
     std::swap(c->U, c->Sa);
   }
@@ -529,7 +557,7 @@ int vt_rhs(vt_ctx* c, double* Udot) {
   if (!c->R) e = alloc(&c->R, sizeof(double2) * 2 * c->Np * static_cast<size_t>(c->Kpad));
   if (!e) e = reset_error_words(c);
   if (!e)
-    e = c->launch(stage_args(c, c->U, c->U, c->A, c->R, vt::kStageRhs, 0.0, 0.0), c->ops.data(), c->grid,
+    e = c->launch(stage_args(c, c->U, c->U, c->A, c->R, vt::kStageRhs, 0.0, 0.0), c->ops.data(),
                   c->stream);
   if (!e) e = soa_to_aos(c, c->R, reinterpret_cast<double*>(c->aos));
   if (!e)
@@ -584,7 +612,7 @@ int vt_profile_rk4_stages(vt_ctx* c, double dt, int reps, float* ms) {
                                    stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6)};
     cudaEventRecord(ev[0], c->stream);
     for (int s = 0; s < 4 && !e; ++s) {
-      e = c->launch(args[s], ops, c->grid, c->stream);
+      e = c->launch(args[s], ops, c->stream);
       cudaEventRecord(ev[s + 1], c->stream);
     }
     if (!e) e = cudaEventSynchronize(ev[4]);
