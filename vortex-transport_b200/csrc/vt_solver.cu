@@ -22,29 +22,36 @@ namespace {
 // Elements per block of the tiled stage kernel (4 threads per element).
 constexpr int kTileElems = 64;
 
-using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, cudaStream_t);
+using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, int, cudaStream_t);
 
-// Opts the instantiation into its dynamic shared memory size; called by
-// vt_create on the context's device, before any launch or graph capture.
+// Opts the instantiation into its dynamic shared memory size and reports how
+// many blocks fit on one SM; called by vt_create on the context's device,
+// before any launch or graph capture.
 template <int P, int NFQ>
-cudaError_t configure_stage() {
+cudaError_t configure_stage(int* blocks_per_sm) {
   using Lay = TileLayout<P, NFQ, kTileElems>;
-  return cudaFuncSetAttribute(tile_stage_kernel<P, NFQ, kTileElems>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
+  cudaError_t e = cudaFuncSetAttribute(tile_stage_kernel<P, NFQ, kTileElems>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
+  if (e) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, tile_stage_kernel<P, NFQ, kTileElems>,
+                                                       4 * kTileElems, Lay::kBytes);
 }
 
+// Persistent launch: at most `max_blocks` blocks (SMs x resident blocks), each
+// walking tiles blockIdx.x, blockIdx.x + gridDim.x, ...
 template <int P, int NFQ>
-cudaError_t launch_stage(const StageArgs& a, const double* ops, cudaStream_t st) {
+cudaError_t launch_stage(const StageArgs& a, const double* ops, int max_blocks, cudaStream_t st) {
   using Lay = TileLayout<P, NFQ, kTileElems>;
   StageOps<P, NFQ> o;
   static_assert(sizeof(StageOps<P, NFQ>) % sizeof(double) == 0, "operator block is doubles");
   std::memcpy(&o, ops, sizeof(o));
-  const int grid = (a.K + kTileElems - 1) / kTileElems;
+  const int ntiles = (a.K + kTileElems - 1) / kTileElems;
+  const int grid = ntiles < max_blocks ? ntiles : max_blocks;
   tile_stage_kernel<P, NFQ, kTileElems><<<grid, 4 * kTileElems, Lay::kBytes, st>>>(a, o);
   return cudaGetLastError();
 }
 
-using ConfigFn = cudaError_t (*)();
+using ConfigFn = cudaError_t (*)(int*);
 
 struct StageKernel {
   LaunchFn launch = nullptr;
@@ -204,6 +211,7 @@ struct vt_ctx {
   std::mutex mu;
   int device = 0, p = 0, Np = 0, nfq = 0, K = 0;
   long long Kpad = 0;
+  int max_blocks = 0;  // persistent grid: SMs x resident blocks per SM
   cudaStream_t stream = nullptr;
   double2 *U = nullptr, *A = nullptr, *Sa = nullptr, *Sb = nullptr, *R = nullptr;
   double2* geo = nullptr;
@@ -262,10 +270,10 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
 cudaError_t enqueue_rk4_step(vt_ctx* c, double dt) {
   cudaError_t e;
   const double* ops = c->ops.data();
-  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2), ops, c->stream))) return e;
-  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2), ops, c->stream))) return e;
-  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt), ops, c->stream))) return e;
-  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6), ops, c->stream);
+  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2), ops, c->max_blocks, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2), ops, c->max_blocks, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt), ops, c->max_blocks, c->stream))) return e;
+  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6), ops, c->max_blocks, c->stream);
 }
 
 cudaError_t reset_error_words(vt_ctx* c) {
@@ -366,11 +374,13 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
   c->Kpad = (static_cast<long long>(K) + 127) / 128 * 128;
   const vt::StageKernel sk = vt::select_kernel(c->p, c->nfq);
   c->launch = sk.launch;
-  if ((e = sk.configure())) {
+  int per_sm = 0, sms = 0;
+  if ((e = sk.configure(&per_sm)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device))) {
     set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
     delete c;
     return nullptr;
   }
+  c->max_blocks = sms * (per_sm > 0 ? per_sm : 1);
   c->ops = vt::fold_operators(c->p, c->nfq, d->inv_mass_ref, d->stiffness_ref, d->line_quadrature,
                               d->phi_plus, d->phi_minus);
 
@@ -535,7 +545,7 @@ int vt_step_euler(vt_ctx* c, double dt, int nsteps) {
   for (int s = 0; s < nsteps && !e; ++s) {
     // double buffer: the neighbours of an element read the old state
     e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, vt::kStageEuler, 0.0, dt), c->ops.data(),
-                  c->stream);
+                  c->max_blocks, c->stream);
     std::swap(c->U, c->Sa);
   }
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("euler", e));
@@ -558,7 +568,7 @@ int vt_rhs(vt_ctx* c, double* Udot) {
   if (!e) e = reset_error_words(c);
   if (!e)
     e = c->launch(stage_args(c, c->U, c->U, c->A, c->R, vt::kStageRhs, 0.0, 0.0), c->ops.data(),
-                  c->stream);
+                  c->max_blocks, c->stream);
   if (!e) e = soa_to_aos(c, c->R, reinterpret_cast<double*>(c->aos));
   if (!e)
     e = cudaMemcpyAsync(Udot, c->aos, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np,
@@ -612,7 +622,7 @@ int vt_profile_rk4_stages(vt_ctx* c, double dt, int reps, float* ms) {
                                    stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6)};
     cudaEventRecord(ev[0], c->stream);
     for (int s = 0; s < 4 && !e; ++s) {
-      e = c->launch(args[s], ops, c->stream);
+      e = c->launch(args[s], ops, c->max_blocks, c->stream);
       cudaEventRecord(ev[s + 1], c->stream);
     }
     if (!e) e = cudaEventSynchronize(ev[4]);

@@ -1,12 +1,16 @@
 // The fused RK stage kernel, tiled through shared memory.
 //
-// One block advances a tile of E consecutive elements through one stage of
-// the nodal DG scheme (Evolve.cpp:135-308, numerical_flux Numericalflux.cpp:13-157,
-// stage update Timestepping.cpp:85-306 / :39-82). The state crosses HBM once:
+// A persistent block walks tiles of E consecutive elements and advances each
+// through one stage of the nodal DG scheme (Evolve.cpp:135-308,
+// numerical_flux Numericalflux.cpp:13-157, stage update Timestepping.cpp:85-306
+// / :39-82). The state crosses HBM once per stage:
 //
-//   1. load   the tile's state (2*Np double2 rows x E, coalesced), the
-//             neighbours across side 0 (their p+1 side nodes) and the
-//             neighbour table into shared memory;
+//   0. prefetch (TMA bulk prefetch into L2) the next tile's state rows,
+//             geometry and neighbour table, and this tile's RK base and
+//             accumulator rows, so the dependent loads below hit L2;
+//   1. load   the tile's state (2*Np double2 rows x E), the neighbours across
+//             side 0 (their p+1 side nodes) and the neighbour table into
+//             shared memory;
 //   2. faces  one work item per (edge, Gauss point). An edge between two tile
 //             elements is evaluated once, by the element with the smaller
 //             index, and its flux is written to both elements' slots (the
@@ -14,12 +18,14 @@
 //             normal being -n); an edge leaving the tile is evaluated by each
 //             side, as in the reference;
 //   3. lift   4 threads per element, one conserved component each: surface
-//             term -(len_s/detJ) LIFT_s F_s into 10 accumulators;
-//   4. flux   the nodal Euler flux, contracted with the inverse Jacobian, of
-//             every node, once, into shared memory;
+//             term -(len_s/detJ) LIFT_s F_s into Np accumulators;
+//   4. flux   the nodal Euler flux of every node, contracted with the inverse
+//             Jacobian, once, into shared memory;
 //   5. volume D_xi G_xi + D_eta G_eta, then the RK stage update written back.
 //
 // The reference's mass-inverse apply is folded into D and LIFT on the host.
+// Shared-memory rows are padded by one element so that rows that differ by a
+// multiple of 128 bytes do not fall into the same banks.
 #pragma once
 
 #include "vt_device.cuh"
@@ -32,24 +38,68 @@ template <int P, int NFQ, int E>
 struct TileLayout {
   static constexpr int NP = np_of_p(P);
   static constexpr int NE = P + 1;
+  static constexpr int ES = E + 1;  // padded row length (elements)
+  static constexpr int kFBDoubles = (3 * 4 * NFQ > NP * 8 ? 3 * 4 * NFQ : NP * 8) * ES;
   // byte offsets into dynamic shared memory, each 16-byte aligned
-  static constexpr int kS = 0;                                        // double2 [2NP][E]
-  static constexpr int kH = align16(kS + 2 * NP * E * 16);            // double2 [2NE][E]
-  static constexpr int kFB = align16(kH + 2 * NE * E * 16);           // double [3][NFQ][4][E] | [NP][8][E]
-  static constexpr int kFBBytes = (3 * NFQ * 4 > NP * 8 ? 3 * NFQ * 4 : NP * 8) * E * 8;
-  static constexpr int kTP = align16(kFB + kFBBytes);                 // double [3][NFQ][NE]
-  static constexpr int kTM = align16(kTP + 3 * NFQ * NE * 8);         // double [3][NFQ][NE]
-  static constexpr int kNB = align16(kTM + 3 * NFQ * NE * 8);         // int4 [E]
-  static constexpr int kItems = align16(kNB + E * 16);                // int [3E]
-  static constexpr int kCount = align16(kItems + 3 * E * 4);          // int [32]
+  static constexpr int kS = 0;                                   // double2 [2NP][ES]
+  static constexpr int kH = align16(kS + 2 * NP * ES * 16);      // double2 [2NE][ES]
+  static constexpr int kFB = align16(kH + 2 * NE * ES * 16);     // double [3][4][NFQ][ES] | [NP][8][ES]
+  static constexpr int kTP = align16(kFB + kFBDoubles * 8);      // double [3][NFQ][NE]
+  static constexpr int kTM = align16(kTP + 3 * NFQ * NE * 8);    // double [3][NFQ][NE]
+  static constexpr int kNB = align16(kTM + 3 * NFQ * NE * 8);    // int4 [E]
+  static constexpr int kItems = align16(kNB + E * 16);           // int [3E]
+  static constexpr int kCount = align16(kItems + 3 * E * 4);     // int [32]
   static constexpr int kBytes = align16(kCount + 32 * 4);
 };
 
+// L2 prefetch of [p, p + bytes) through the TMA unit; bytes is a multiple of
+// 16 and p is 16-byte aligned (every row start of the SoA layout is).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+template <int NP, int E>
+__device__ __forceinline__ void prefetch_tile(const StageArgs& a, int tile, bool current, int t) {
+  const int e0 = tile * E;
+  const int ne = min(E, a.K - e0);
+  if (ne <= 0) return;
+  const unsigned bytes = static_cast<unsigned>(ne) * 16u;
+  const long long KP = a.Kpad;
+  int r = t;
+  if (!current) {
+    // the next tile: stage input rows, geometry rows, neighbour table
+    if (r < 2 * NP) {
+      prefetch_l2(a.in + r * KP + e0, bytes);
+      return;
+    }
+    r -= 2 * NP;
+    if (r < 7) {
+      prefetch_l2(a.geo + r * KP + e0, bytes);
+      return;
+    }
+    r -= 7;
+    if (r == 0) prefetch_l2(a.nbr + e0, bytes);
+    return;
+  }
+  // this tile: rows the stage update reads at the end
+  const bool want_base = a.stage == 1 || a.stage == 2;
+  const bool want_acc = a.stage >= 1 && a.stage <= 3;
+  if (r < 2 * NP) {
+    if (want_acc) prefetch_l2(a.acc + r * KP + e0, bytes);
+    return;
+  }
+  r -= 2 * NP;
+  if (r < 2 * NP && want_base) prefetch_l2(a.base + r * KP + e0, bytes);
+}
+
 template <int P, int NFQ, int E>
-__global__ void __launch_bounds__(4 * E) tile_stage_kernel(const StageArgs a, const StageOps<P, NFQ> ops) {
+// Three 256-thread blocks per SM (<= 80 registers per thread) keep 24 warps
+// resident alongside 3 x ~73 KB of shared memory.
+__global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a, const StageOps<P, NFQ> ops) {
   using L = TileLayout<P, NFQ, E>;
   constexpr int NP = L::NP;
   constexpr int NE = L::NE;
+  constexpr int ES = L::ES;
   constexpr int T = 4 * E;
   extern __shared__ __align__(16) unsigned char smem[];
   double2* S = reinterpret_cast<double2*>(smem + L::kS);
@@ -62,25 +112,10 @@ __global__ void __launch_bounds__(4 * E) tile_stage_kernel(const StageArgs a, co
   int* counts = reinterpret_cast<int*>(smem + L::kCount);
 
   const int t = threadIdx.x;
-  const int e0 = blockIdx.x * E;
   const long long KP = a.Kpad;
+  const int ntiles = (a.K + E - 1) / E;
 
-  // ---- 1. load ---------------------------------------------------------------
   {
-    const int col = t % E, grp = t / E;
-    const int e = e0 + col;
-    const bool valid = e < a.K;
-    int4 nb = make_int4(e, e, e, 0);
-    if (valid) nb = __ldg(a.nbr + e);
-    if (grp == 0) NB[col] = nb;
-#pragma unroll
-    for (int r = grp; r < 2 * NP; r += 4)
-      S[r * E + col] = valid ? __ldg(a.in + r * KP + e) : make_double2(1.0, 0.0);
-#pragma unroll
-    for (int r = grp; r < 2 * NE; r += 4) {
-      // side 0 nodes are nodes 0..P: rows 0..2P+1
-      H[r * E + col] = valid ? __ldg(a.in + r * KP + nb.x) : make_double2(1.0, 0.0);
-    }
     const double* tp = &ops.tp[0][0][0];
     const double* tm = &ops.tm[0][0][0];
     for (int l = t; l < 3 * NFQ * NE; l += T) {
@@ -88,180 +123,213 @@ __global__ void __launch_bounds__(4 * E) tile_stage_kernel(const StageArgs a, co
       TM[l] = tm[l];
     }
   }
-  __syncthreads();
 
-  // ---- edge list: (element, side) pairs this tile evaluates ------------------
-  {
-    const int lane = t & 31, warp = t >> 5;
-    bool take = false;
-    int code = 0;
-    if (t < 3 * E) {
-      const int el = t / 3, s = t % 3;
-      if (e0 + el < a.K) {
-        const int4 nb4 = NB[el];
-        const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
-        const int nl = nb - e0;
-        const bool inside = nl >= 0 && nl < E;
-        take = !inside || (e0 + el < nb);
-        code = el | (s << 8) | ((inside && nb != e0 + el) ? (1 << 10) : 0);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = tile * E;
+
+    // ---- 0. prefetch ------------------------------------------------------------
+    if (t < 32) {
+      if (tile + gridDim.x < ntiles) prefetch_tile<NP, E>(a, tile + gridDim.x, false, t);
+    } else if (t < 32 + 4 * NP) {
+      prefetch_tile<NP, E>(a, tile, true, t - 32);
+    }
+
+    // ---- 1. load ------------------------------------------------------------------
+    {
+      const int col = t % E, grp = t / E;
+      const int e = e0 + col;
+      const bool valid = e < a.K;
+      int4 nb = make_int4(e, e, e, 0);
+      if (valid) nb = __ldg(a.nbr + e);
+      if (grp == 0) NB[col] = nb;
+#pragma unroll
+      for (int r = grp; r < 2 * NP; r += 4)
+        S[r * ES + col] = valid ? __ldg(a.in + r * KP + e) : make_double2(1.0, 0.0);
+#pragma unroll
+      for (int r = grp; r < 2 * NE; r += 4)  // side 0 nodes are nodes 0..P: rows 0..2P+1
+        H[r * ES + col] = valid ? __ldg(a.in + r * KP + nb.x) : make_double2(1.0, 0.0);
+    }
+    __syncthreads();
+
+    // ---- edge list: (element, side) pairs this tile evaluates ----------------------
+    {
+      const int lane = t & 31, warp = t >> 5;
+      bool take = false;
+      int code = 0;
+      if (t < 3 * E) {
+        const int el = t / 3, s = t % 3;
+        if (e0 + el < a.K) {
+          const int4 nb4 = NB[el];
+          const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
+          const int nl = nb - e0;
+          const bool inside = nl >= 0 && nl < E;
+          take = !inside || (e0 + el < nb);
+          code = el | (s << 8) | ((inside && nb != e0 + el) ? (1 << 10) : 0);
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (lane == 0) counts[warp] = __popc(m);
+      __syncthreads();
+      int base = 0;
+      for (int w = 0; w < warp; ++w) base += counts[w];
+      if (take) items[base + __popc(m & ((1u << lane) - 1u))] = code;
+      if (t == 0) {
+        int n = 0;
+        for (int w = 0; w < T / 32; ++w) n += counts[w];
+        counts[T / 32] = n;
+      }
+      __syncthreads();
+    }
+    const int nitems = counts[T / 32];
+
+    // ---- 2. faces ----------------------------------------------------------------------
+    for (int w = t; w < nitems * NFQ; w += T) {
+      const int it = items[w / NFQ];
+      const int q = w % NFQ;
+      const int el = it & 0xff, s = (it >> 8) & 3;
+      const bool mirror = (it >> 10) & 1;
+      const int e = e0 + el;
+      const int4 nb4 = NB[el];
+      const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
+      const int nl = nb - e0;
+      const bool inside = nl >= 0 && nl < E;
+      double up[4] = {0, 0, 0, 0}, um[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int k = 0; k < NE; ++k) {
+        const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
+        const double cp = TP[(s * NFQ + q) * NE + k];
+        const double cm = TM[(s * NFQ + q) * NE + k];
+        const double2 o0 = S[(2 * node) * ES + el], o1 = S[(2 * node + 1) * ES + el];
+        double2 n0, n1;
+        if (inside) {
+          n0 = S[(2 * node) * ES + nl];
+          n1 = S[(2 * node + 1) * ES + nl];
+        } else if (s == 0) {
+          n0 = H[(2 * k) * ES + el];
+          n1 = H[(2 * k + 1) * ES + el];
+        } else {
+          n0 = __ldg(a.in + (2 * node) * KP + nb);
+          n1 = __ldg(a.in + (2 * node + 1) * KP + nb);
+        }
+        up[0] += cp * o0.x;
+        up[1] += cp * o0.y;
+        up[2] += cp * o1.x;
+        up[3] += cp * o1.y;
+        um[0] += cm * n0.x;
+        um[1] += cm * n0.y;
+        um[2] += cm * n1.x;
+        um[3] += cm * n1.y;
+      }
+      const double2 n = __ldg(a.geo + (2 + s) * KP + e);
+      double f[4];
+      const int code = roe_flux(up, um, n.x, n.y, f);
+      if (code) record_error(a, NFQ, e, q, s, code);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + q) * ES + el] = f[c];
+      if (mirror) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + (NFQ - 1 - q)) * ES + nl] = -f[c];
       }
     }
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    if (lane == 0) counts[warp] = __popc(m);
     __syncthreads();
-    int base = 0;
-    for (int w = 0; w < warp; ++w) base += counts[w];
-    if (take) items[base + __popc(m & ((1u << lane) - 1u))] = code;
-    __syncthreads();
-    if (t == 0) {
-      int n = 0;
-      for (int w = 0; w < T / 32; ++w) n += counts[w];
-      counts[T / 32] = n;
-    }
-    __syncthreads();
-  }
-  const int nitems = counts[T / 32];
 
-  // ---- 2. faces ------------------------------------------------------------------
-  for (int w = t; w < nitems * NFQ; w += T) {
-    const int it = items[w / NFQ];
-    const int q = w % NFQ;
-    const int el = it & 0xff, s = (it >> 8) & 3;
-    const bool mirror = (it >> 10) & 1;
+    // ---- 3. lift: thread (element el, component c) --------------------------------------
+    const int c = t / E;  // uniform per warp
+    const int el = t % E;
     const int e = e0 + el;
-    const int4 nb4 = NB[el];
-    const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
-    const int nl = nb - e0;
-    const bool inside = nl >= 0 && nl < E;
-    double up[4] = {0, 0, 0, 0}, um[4] = {0, 0, 0, 0};
+    const bool valid = e < a.K;
+    const int eg = valid ? e : e0;
+    double r[NP];
 #pragma unroll
-    for (int k = 0; k < NE; ++k) {
-      const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
-      const double cp = TP[(s * NFQ + q) * NE + k];
-      const double cm = TM[(s * NFQ + q) * NE + k];
-      const double2 o0 = S[(2 * node) * E + el], o1 = S[(2 * node + 1) * E + el];
-      double2 n0, n1;
-      if (inside) {
-        n0 = S[(2 * node) * E + nl];
-        n1 = S[(2 * node + 1) * E + nl];
-      } else if (s == 0) {
-        n0 = H[(2 * k) * E + el];
-        n1 = H[(2 * k + 1) * E + el];
-      } else {
-        n0 = __ldg(a.in + (2 * node) * KP + nb);
-        n1 = __ldg(a.in + (2 * node + 1) * KP + nb);
-      }
-      up[0] += cp * o0.x;
-      up[1] += cp * o0.y;
-      up[2] += cp * o1.x;
-      up[3] += cp * o1.y;
-      um[0] += cm * n0.x;
-      um[1] += cm * n0.y;
-      um[2] += cm * n1.x;
-      um[3] += cm * n1.y;
-    }
-    const double2 n = __ldg(a.geo + (2 + s) * KP + e);
-    double f[4];
-    const int code = roe_flux(up, um, n.x, n.y, f);
-    if (code) record_error(a, NFQ, e, q, s, code);
+    for (int i = 0; i < NP; ++i) r[i] = 0.0;
+    {
+      const double2 lsa = __ldg(a.geo + 5 * KP + eg);
+      const double2 lsb = __ldg(a.geo + 6 * KP + eg);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) FB[((s * NFQ + q) * 4 + c) * E + el] = f[c];
-    if (mirror) {
+      for (int s = 0; s < 3; ++s) {
+        const double ls = s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) FB[((s * NFQ + (NFQ - 1 - q)) * 4 + c) * E + nl] = -f[c];
-    }
-  }
-  __syncthreads();
-
-  // ---- 3. lift: thread (element el, component c) ----------------------------------
-  const int c = t / E;  // uniform per warp
-  const int el = t % E;
-  const int e = e0 + el;
-  const bool valid = e < a.K;
-  double r[NP];
+        for (int q = 0; q < NFQ; ++q) {
+          const double fs = ls * FB[((s * 4 + c) * NFQ + q) * ES + el];
 #pragma unroll
-  for (int i = 0; i < NP; ++i) r[i] = 0.0;
-  {
-    const double2 lsa = __ldg(a.geo + 5 * KP + (valid ? e : 0));
-    const double2 lsb = __ldg(a.geo + 6 * KP + (valid ? e : 0));
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      const double ls = s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x);
-#pragma unroll
-      for (int q = 0; q < NFQ; ++q) {
-        const double fs = ls * FB[((s * NFQ + q) * 4 + c) * E + el];
-#pragma unroll
-        for (int i = 0; i < NP; ++i) r[i] -= ops.lift[s][i][q] * fs;
-      }
-    }
-  }
-  __syncthreads();
-
-  // ---- 4. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ------
-  double* G = FB;
-  if (P > 0) {
-    const double2 j0 = __ldg(a.geo + 0 * KP + (valid ? e : 0));
-    const double2 j1 = __ldg(a.geo + 1 * KP + (valid ? e : 0));
-#pragma unroll
-    for (int j = c; j < NP; j += 4) {
-      const double2 s0 = S[(2 * j) * E + el], s1 = S[(2 * j + 1) * E + el];
-      const double sv[4] = {s0.x, s0.y, s1.x, s1.y};
-      double gxi[4], geta[4];
-      contravariant_flux(sv, j0.x, j0.y, j1.x, j1.y, gxi, geta);
-#pragma unroll
-      for (int cc = 0; cc < 4; ++cc) {
-        G[(j * 8 + cc) * E + el] = gxi[cc];
-        G[(j * 8 + 4 + cc) * E + el] = geta[cc];
+          for (int i = 0; i < NP; ++i) r[i] -= ops.lift[s][i][q] * fs;
+        }
       }
     }
     __syncthreads();
 
-    // ---- 5a. volume ------------------------------------------------------------------
+    // ---- 4. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ---------------
+    if (P > 0) {
+      double* G = FB;
+      const double2 j0 = __ldg(a.geo + 0 * KP + eg);
+      const double2 j1 = __ldg(a.geo + 1 * KP + eg);
+      for (int j = c; j < NP; j += 4) {
+        const double2 s0 = S[(2 * j) * ES + el], s1 = S[(2 * j + 1) * ES + el];
+        const double sv[4] = {s0.x, s0.y, s1.x, s1.y};
+        double gxi[4], geta[4];
+        contravariant_flux(sv, j0.x, j0.y, j1.x, j1.y, gxi, geta);
 #pragma unroll
-    for (int j = 0; j < NP; ++j) {
-      const double gx = G[(j * 8 + c) * E + el];
-      const double gy = G[(j * 8 + 4 + c) * E + el];
-#pragma unroll
-      for (int i = 0; i < NP; ++i) r[i] += ops.D[0][i][j] * gx + ops.D[1][i][j] * gy;
-    }
-  }
+        for (int cc = 0; cc < 4; ++cc) {
+          G[(j * 8 + cc) * ES + el] = gxi[cc];
+          G[(j * 8 + 4 + cc) * ES + el] = geta[cc];
+        }
+      }
+      __syncthreads();
 
-  // ---- 5b. stage update: component c of every node ------------------------------------
-  if (valid) {
-    const int h = c >> 1, part = c & 1;
-    const double* base = reinterpret_cast<const double*>(a.base);
-    double* acc = reinterpret_cast<double*>(a.acc);
-    double* out = reinterpret_cast<double*>(a.out);
+      // ---- 5a. volume ------------------------------------------------------------------
 #pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      const long long idx = (((2 * i + h) * KP) + e) * 2 + part;
-      const double2 sv = S[(2 * i + h) * E + el];
-      const double u = part ? sv.y : sv.x;
+      for (int j = 0; j < NP; ++j) {
+        const double gx = G[(j * 8 + c) * ES + el];
+        const double gy = G[(j * 8 + 4 + c) * ES + el];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) r[i] += ops.D[0][i][j] * gx + ops.D[1][i][j] * gy;
+      }
+    }
+
+    // ---- 5b. stage update: component c of every node ----------------------------------
+    if (valid) {
+      const int h = c >> 1, part = c & 1;
+      const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
+      const double* base = reinterpret_cast<const double*>(a.base) + off0;
+      double* acc = reinterpret_cast<double*>(a.acc) + off0;
+      double* out = reinterpret_cast<double*>(a.out) + off0;
+      const double* sv = reinterpret_cast<const double*>(S + h * ES + el) + part;
+      const long long step = 4 * KP;  // doubles between node rows of the same pair
       switch (a.stage) {
         case 0:
-          acc[idx] = u + a.c_acc * r[i];
-          out[idx] = u + a.c_out * r[i];
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double u = sv[i * 4 * ES];
+            acc[i * step] = u + a.c_acc * r[i];
+            out[i * step] = u + a.c_out * r[i];
+          }
           break;
         case 1:
         case 2:
-          acc[idx] = acc[idx] + a.c_acc * r[i];
-          out[idx] = __ldg(base + idx) + a.c_out * r[i];
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            acc[i * step] = acc[i * step] + a.c_acc * r[i];
+            out[i * step] = __ldg(base + i * step) + a.c_out * r[i];
+          }
           break;
         case 3:
-          out[idx] = acc[idx] + a.c_out * r[i];
+#pragma unroll
+          for (int i = 0; i < NP; ++i) out[i * step] = acc[i * step] + a.c_out * r[i];
           break;
         case kStageEuler:
-          out[idx] = u + a.c_out * r[i];
+#pragma unroll
+          for (int i = 0; i < NP; ++i) out[i * step] = sv[i * 4 * ES] + a.c_out * r[i];
           break;
         default:
-          out[idx] = r[i];
+#pragma unroll
+          for (int i = 0; i < NP; ++i) out[i * step] = r[i];
           break;
       }
     }
+    __syncthreads();  // the next tile reuses the shared buffers
   }
 
   if (a.stage == 3 || a.stage == kStageEuler) {
-    __syncthreads();
     if (t == 0) {
       __threadfence();
       const unsigned long long done = atomicAdd(&a.err[2], 1ull);
