@@ -188,6 +188,54 @@ void* vt_stream(vt_ctx* ctx);
  * `reps` steps of size dt. Advances the state by `reps` steps. */
 int vt_profile_rk4_stages(vt_ctx* ctx, double dt, int reps, float* ms);
 
+/* ---- stepping without device allocation --------------------------------- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc:
+ * code running while a host framework's pool or arena owns all device memory,
+ * real-time loops where a cudaMalloc or cudaFree would synchronise the device,
+ * and plugins that may only use buffers their host passes in. All scratch
+ * (packed geometry, the state in the kernel's layout, the RK accumulator and
+ * stage buffers, error words) lives in one fixed device array of
+ * VT_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the
+ * library holds until the process exits. */
+#define VT_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* vt_mesh_desc with the per-element arrays in DEVICE memory (same layouts);
+ * the reference-space tables stay in host memory. */
+typedef struct vt_device_mesh {
+  int32_t p;
+  int32_t n_elements;
+  int32_t n_line_points;
+  const int32_t* element_type;   /* device, K */
+  const int32_t* neighbours;     /* device, K x 3: right, left, vertical */
+  const double* det_jacobian;    /* device, K */
+  const double* inv_jacobian;    /* device, K x 4 */
+  const double* normals;         /* device, K x 3 x 2 */
+  const double* side_lengths;    /* device, K x 3 */
+  const double* inv_mass_ref;    /* host, Np x Np */
+  const double* stiffness_ref;   /* host, 2 x Np x Np */
+  const double* line_quadrature; /* host, nfq x 2 */
+  const double* phi_plus;        /* host, 3 x Np x nfq */
+  const double* phi_minus;       /* host, 3 x Np x nfq */
+} vt_device_mesh;
+
+/* Bytes of the fixed scratch a problem of this size needs (0 if p is out of
+ * range); problems needing more than VT_NOALLOC_SCRATCH_BYTES are rejected. At
+ * p = 3 that is about 11,900 elements. */
+size_t vt_noalloc_scratch_bytes(int p, int n_elements);
+
+/* nsteps RK4 steps from dU_in to dU_out (device, K x Np x 4, the reference
+ * layout; they may be the same buffer) on `stream` (a cudaStream_t, NULL for
+ * the default stream), the same kernels as vt_step_rk4, with no cudaMalloc,
+ * cudaFree or allocating library call. Blocks until done. Returns VT_OK, a
+ * non-physical-state code with `err` filled in, VT_ERR_INVALID for a problem
+ * larger than the scratch or a bad neighbour index, or VT_ERR_CUDA.
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current, so make that first call
+ * before any stream capture. Every call shares the one array and leaves its
+ * contents behind; calls whose work overlaps on the GPU race on it. */
+int vt_step_rk4_noalloc(const vt_device_mesh* mesh, const double* dU_in, double* dU_out, double dt,
+                        int nsteps, void* stream, vt_error_info* err);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,16 @@ class vt_error_info(ctypes.Structure):
                 ("side", ctypes.c_int), ("step", ctypes.c_int64), ("stage", ctypes.c_int)]
 
 
+class vt_device_mesh(ctypes.Structure):
+    """vt_mesh_desc with the per-element arrays in device memory."""
+    _fields_ = [("p", ctypes.c_int32), ("n_elements", ctypes.c_int32),
+                ("n_line_points", ctypes.c_int32), ("element_type", ctypes.c_void_p),
+                ("neighbours", ctypes.c_void_p), ("det_jacobian", ctypes.c_void_p),
+                ("inv_jacobian", ctypes.c_void_p), ("normals", ctypes.c_void_p),
+                ("side_lengths", ctypes.c_void_p), ("inv_mass_ref", _dp), ("stiffness_ref", _dp),
+                ("line_quadrature", _dp), ("phi_plus", _dp), ("phi_minus", _dp)]
+
+
 class VortexError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"[{status}] {message}")
@@ -130,6 +140,10 @@ _SIGNATURES = {
     "vt_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "vt_profile_rk4_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_float)]),
+    "vt_noalloc_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
+    "vt_step_rk4_noalloc": (ctypes.c_int, [ctypes.POINTER(vt_device_mesh), ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.POINTER(vt_error_info)]),
 }
 
 
