@@ -220,7 +220,7 @@ typedef struct vt_device_mesh {
 
 /* Bytes of the fixed scratch a problem of this size needs (0 if p is out of
  * range); problems needing more than VT_NOALLOC_SCRATCH_BYTES are rejected. At
- * p = 3 that is about 11,900 elements. */
+ * p = 3 that is about 11,700 elements. */
 size_t vt_noalloc_scratch_bytes(int p, int n_elements);
 
 /* nsteps RK4 steps from dU_in to dU_out (device, K x Np x 4, the reference

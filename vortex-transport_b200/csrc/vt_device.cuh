@@ -50,6 +50,12 @@ struct StageOps {
 //   0: (Jinv00, Jinv01)  1: (Jinv10, Jinv11)  2..4: normal of side 0..2
 //   5: (len0/detJ, len1/detJ)  6: (len2/detJ, 0)
 // nbr[e] = (neighbour across side 0, 1, 2, unused).
+//
+// Tiles: tiles[t] = (start0, len0, start1, len1), two runs of consecutive
+// elements (local columns 0..31 and 32..63). tile_items[t * kMaxItems + i],
+// i < tile_count[t], lists the (element, side) faces tile t evaluates:
+//   bits 0-7 local element, 8-9 side, 10 mirror (the neighbour is in the tile
+//   and receives -F), 11-18 the neighbour's local column when mirrored.
 struct StageArgs {
   const double2* in;    // state the right-hand side is evaluated on
   const double2* base;  // U_n (RK4 stages 1, 2)
@@ -57,13 +63,21 @@ struct StageArgs {
   double2* out;         // next stage state / new U / the right-hand side itself
   const double2* geo;
   const int4* nbr;
+  const int4* tiles;
+  const int* tile_items;
+  const int* tile_count;
   unsigned long long* err;  // [0] first-error key, [1] steps done, [2] blocks done
   long long Kpad;
   int K;
+  int ntiles;
   int stage;     // 0..3 RK4 stages, 4 forward Euler, 5 right-hand side only
   double c_acc;  // accumulator coefficient
   double c_out;  // output coefficient
 };
+
+constexpr int kTileRun = 32;            // elements per run
+constexpr int kTileElems = 2 * kTileRun;  // elements per tile
+constexpr int kMaxItems = 3 * kTileElems;
 
 enum : int { kStageEuler = 4, kStageRhs = 5 };
 

@@ -1,0 +1,38 @@
+// Dispatch to the stage kernel instantiation for (p, nfq), and the tile
+// schedule builders; one translation unit (vt_launch.cu) instantiates them.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "vt_device.cuh"
+
+namespace vt {
+
+using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, int, cudaStream_t);
+using ConfigFn = cudaError_t (*)(int*);
+
+struct StageKernel {
+  // Launches one stage with at most `max_blocks` persistent blocks.
+  LaunchFn launch = nullptr;
+  // Sets the dynamic shared-memory attribute on the current device and
+  // reports resident blocks per SM. Call before any launch or capture.
+  ConfigFn configure = nullptr;
+};
+
+// Empty (null members) for p outside 0..3 or nfq outside 1..10.
+StageKernel select_kernel(int p, int nfq);
+
+// Number of doubles of the StageOps<P, NFQ> block for (p, nfq).
+int stage_ops_doubles(int p, int nfq);
+
+// Two-row tiles for the reference's structured mesh, empty if `conn` is not it.
+std::vector<int4> structured_tile_runs(int K, const int32_t* type, const int32_t* conn);
+
+// Device-side: tiles of 64 consecutive elements, then the per-tile face lists.
+cudaError_t launch_contiguous_tiles(int4* tiles, int K, int ntiles, cudaStream_t st);
+cudaError_t launch_build_tile_items(const int4* tiles, const int4* nbr, int* items, int* count, int ntiles,
+                                    cudaStream_t st);
+
+}  // namespace vt

@@ -6,7 +6,7 @@
 // framework), real-time loops where a cudaMalloc/cudaFree would synchronise
 // the device and stall the loop, and plugins that are only allowed to touch
 // buffers their host passes in. For them this file keeps the stepper's
-// scratch -- the packed geometry and neighbour rows, the state in the
+// scratch -- the packed geometry and neighbour rows, the tile schedule, the state in the
 // kernel's layout, the RK accumulator, the two stage buffers and the error
 // words -- in one file-scope __device__ array of kScratchBytes, which every
 // GPU that loads the library holds until the process exits. The caller passes
@@ -25,13 +25,12 @@
 #include "../../include/vortex_b200.h"
 #include "vt_common.h"
 #include "vt_precompute.h"
-#include "vt_tile.cuh"
+#include "vt_launch.h"
 
 namespace vt {
 namespace {
 
 constexpr size_t kScratchBytes = VT_NOALLOC_SCRATCH_BYTES;
-constexpr int kTileE = 64;
 constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
@@ -51,7 +50,8 @@ size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
 struct Carve {
   long long Kpad;
-  size_t err, geo, nbr, U, A, Sa, Sb, total;
+  int ntiles;
+  size_t err, geo, nbr, tiles, items, count, U, A, Sa, Sb, total;
 };
 
 Carve carve(int p, int K) {
@@ -61,7 +61,11 @@ Carve carve(int p, int K) {
   c.err = 0;
   c.geo = align256(c.err + 4 * sizeof(unsigned long long));
   c.nbr = align256(c.geo + sizeof(double2) * 7 * static_cast<size_t>(c.Kpad));
-  c.U = align256(c.nbr + sizeof(int4) * static_cast<size_t>(c.Kpad));
+  c.ntiles = (K + kTileElems - 1) / kTileElems;
+  c.tiles = align256(c.nbr + sizeof(int4) * static_cast<size_t>(c.Kpad));
+  c.items = align256(c.tiles + sizeof(int4) * static_cast<size_t>(c.ntiles));
+  c.count = align256(c.items + sizeof(int) * kMaxItems * static_cast<size_t>(c.ntiles));
+  c.U = align256(c.count + sizeof(int) * static_cast<size_t>(c.ntiles));
   c.A = align256(c.U + state);
   c.Sa = align256(c.A + state);
   c.Sb = align256(c.Sa + state);
@@ -107,62 +111,6 @@ __global__ void scatter_aos_kernel(const double2* __restrict__ soa, double2* __r
   if (l >= static_cast<long long>(K) * 2 * Np) return;
   const int r = static_cast<int>(l / K), e = static_cast<int>(l % K);
   aos[static_cast<long long>(e) * 2 * Np + r] = soa[r * KP + e];
-}
-
-using Launch = cudaError_t (*)(const StageArgs&, const double*, int, cudaStream_t);
-using Config = cudaError_t (*)(int*);
-
-template <int P, int NFQ>
-cudaError_t config_noalloc(int* per_sm) {
-  using Lay = TileLayout<P, NFQ, kTileE>;
-  cudaError_t e = cudaFuncSetAttribute(tile_stage_kernel<P, NFQ, kTileE>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
-  if (e) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, tile_stage_kernel<P, NFQ, kTileE>, 4 * kTileE,
-                                                       Lay::kBytes);
-}
-
-template <int P, int NFQ>
-cudaError_t launch_noalloc(const StageArgs& a, const double* ops, int max_blocks, cudaStream_t st) {
-  using Lay = TileLayout<P, NFQ, kTileE>;
-  StageOps<P, NFQ> o;
-  std::memcpy(&o, ops, sizeof(o));
-  const int ntiles = (a.K + kTileE - 1) / kTileE;
-  tile_stage_kernel<P, NFQ, kTileE><<<ntiles < max_blocks ? ntiles : max_blocks, 4 * kTileE, Lay::kBytes, st>>>(
-      a, o);
-  return cudaGetLastError();
-}
-
-struct Pick {
-  Launch launch = nullptr;
-  Config config = nullptr;
-};
-
-template <int P>
-Pick pick_nfq(int nfq) {
-  switch (nfq) {
-    case 1: return {launch_noalloc<P, 1>, config_noalloc<P, 1>};
-    case 2: return {launch_noalloc<P, 2>, config_noalloc<P, 2>};
-    case 3: return {launch_noalloc<P, 3>, config_noalloc<P, 3>};
-    case 4: return {launch_noalloc<P, 4>, config_noalloc<P, 4>};
-    case 5: return {launch_noalloc<P, 5>, config_noalloc<P, 5>};
-    case 6: return {launch_noalloc<P, 6>, config_noalloc<P, 6>};
-    case 7: return {launch_noalloc<P, 7>, config_noalloc<P, 7>};
-    case 8: return {launch_noalloc<P, 8>, config_noalloc<P, 8>};
-    case 9: return {launch_noalloc<P, 9>, config_noalloc<P, 9>};
-    case 10: return {launch_noalloc<P, 10>, config_noalloc<P, 10>};
-    default: return {};
-  }
-}
-
-Pick pick(int p, int nfq) {
-  switch (p) {
-    case 0: return pick_nfq<0>(nfq);
-    case 1: return pick_nfq<1>(nfq);
-    case 2: return pick_nfq<2>(nfq);
-    case 3: return pick_nfq<3>(nfq);
-    default: return {};
-  }
 }
 
 // The operator block of StageOps<P, NFQ> (at most 740 doubles), folded on the
@@ -223,7 +171,7 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: the problem needs " + std::to_string(cv.total) +
                                     " bytes of scratch, more than the fixed " +
                                     std::to_string(vt::kScratchBytes) + " (use vt_create for larger meshes)");
-  const vt::Pick pk = vt::pick(m->p, m->n_line_points);
+  const vt::StageKernel pk = vt::select_kernel(m->p, m->n_line_points);
 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -243,13 +191,16 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     }
   }
   int per_sm = 0;
-  if ((e = pk.config(&per_sm))) return fail(VT_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
+  if ((e = pk.configure(&per_sm))) return fail(VT_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
   const int max_blocks = ds->sms * (per_sm > 0 ? per_sm : 1);
 
   unsigned char* base = ds->scratch;
   auto* errw = reinterpret_cast<unsigned long long*>(base + cv.err);
   auto* geo = reinterpret_cast<double2*>(base + cv.geo);
   auto* nbr = reinterpret_cast<int4*>(base + cv.nbr);
+  auto* tiles = reinterpret_cast<int4*>(base + cv.tiles);
+  auto* items = reinterpret_cast<int*>(base + cv.items);
+  auto* count = reinterpret_cast<int*>(base + cv.count);
   auto* U = reinterpret_cast<double2*>(base + cv.U);
   auto* A = reinterpret_cast<double2*>(base + cv.A);
   auto* Sa = reinterpret_cast<double2*>(base + cv.Sa);
@@ -265,6 +216,9 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
       (e = cudaMemsetAsync(errw + 1, 0, 3 * sizeof(unsigned long long), st)))
     return fail(VT_ERR_CUDA, std::string("scratch reset: ") + cudaGetErrorString(e));
   vt::pack_geometry_kernel<<<(K + 255) / 256, 256, 0, st>>>(*m, geo, nbr, cv.Kpad, errw);
+  if ((e = vt::launch_contiguous_tiles(tiles, K, cv.ntiles, st)) ||
+      (e = vt::launch_build_tile_items(tiles, nbr, items, count, cv.ntiles, st)))
+    return fail(VT_ERR_CUDA, std::string("tile schedule: ") + cudaGetErrorString(e));
   const long long nrow = static_cast<long long>(K) * 2 * Np;
   const int tb = static_cast<int>((nrow + 255) / 256);
   vt::gather_soa_kernel<<<tb, 256, 0, st>>>(reinterpret_cast<const double2*>(dU_in), U, K, Np, cv.Kpad);
@@ -278,6 +232,10 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     a.out = out;
     a.geo = geo;
     a.nbr = nbr;
+    a.tiles = tiles;
+    a.tile_items = items;
+    a.tile_count = count;
+    a.ntiles = cv.ntiles;
     a.err = errw;
     a.Kpad = cv.Kpad;
     a.K = K;

@@ -14,81 +14,10 @@
 #include "../../include/vortex_b200.h"
 #include "vt_common.h"
 #include "vt_precompute.h"
-#include "vt_tile.cuh"
+#include "vt_launch.h"
 
 namespace vt {
 namespace {
-
-// Elements per block of the tiled stage kernel (4 threads per element).
-constexpr int kTileElems = 64;
-
-using LaunchFn = cudaError_t (*)(const StageArgs&, const double*, int, cudaStream_t);
-
-// Opts the instantiation into its dynamic shared memory size and reports how
-// many blocks fit on one SM; called by vt_create on the context's device,
-// before any launch or graph capture.
-template <int P, int NFQ>
-cudaError_t configure_stage(int* blocks_per_sm) {
-  using Lay = TileLayout<P, NFQ, kTileElems>;
-  cudaError_t e = cudaFuncSetAttribute(tile_stage_kernel<P, NFQ, kTileElems>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
-  if (e) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, tile_stage_kernel<P, NFQ, kTileElems>,
-                                                       4 * kTileElems, Lay::kBytes);
-}
-
-// Persistent launch: at most `max_blocks` blocks (SMs x resident blocks), each
-// walking tiles blockIdx.x, blockIdx.x + gridDim.x, ...
-template <int P, int NFQ>
-cudaError_t launch_stage(const StageArgs& a, const double* ops, int max_blocks, cudaStream_t st) {
-  using Lay = TileLayout<P, NFQ, kTileElems>;
-  StageOps<P, NFQ> o;
-  static_assert(sizeof(StageOps<P, NFQ>) % sizeof(double) == 0, "operator block is doubles");
-  std::memcpy(&o, ops, sizeof(o));
-  const int ntiles = (a.K + kTileElems - 1) / kTileElems;
-  const int grid = ntiles < max_blocks ? ntiles : max_blocks;
-  tile_stage_kernel<P, NFQ, kTileElems><<<grid, 4 * kTileElems, Lay::kBytes, st>>>(a, o);
-  return cudaGetLastError();
-}
-
-using ConfigFn = cudaError_t (*)(int*);
-
-struct StageKernel {
-  LaunchFn launch = nullptr;
-  ConfigFn configure = nullptr;
-};
-
-template <int P, int NFQ>
-StageKernel stage_kernel_of() {
-  return StageKernel{launch_stage<P, NFQ>, configure_stage<P, NFQ>};
-}
-
-template <int P>
-StageKernel kernel_for_nfq(int nfq) {
-  switch (nfq) {
-    case 1: return stage_kernel_of<P, 1>();
-    case 2: return stage_kernel_of<P, 2>();
-    case 3: return stage_kernel_of<P, 3>();
-    case 4: return stage_kernel_of<P, 4>();
-    case 5: return stage_kernel_of<P, 5>();
-    case 6: return stage_kernel_of<P, 6>();
-    case 7: return stage_kernel_of<P, 7>();
-    case 8: return stage_kernel_of<P, 8>();
-    case 9: return stage_kernel_of<P, 9>();
-    case 10: return stage_kernel_of<P, 10>();
-    default: return StageKernel{};
-  }
-}
-
-StageKernel select_kernel(int p, int nfq) {
-  switch (p) {
-    case 0: return kernel_for_nfq<0>(nfq);
-    case 1: return kernel_for_nfq<1>(nfq);
-    case 2: return kernel_for_nfq<2>(nfq);
-    case 3: return kernel_for_nfq<3>(nfq);
-    default: return StageKernel{};
-  }
-}
 
 // Folds M_ref^-1 into the volume and lift operators and restricts the face
 // tables to each side's nodes, in the layout of StageOps<P, NFQ>.
@@ -216,6 +145,10 @@ struct vt_ctx {
   double2 *U = nullptr, *A = nullptr, *Sa = nullptr, *Sb = nullptr, *R = nullptr;
   double2* geo = nullptr;
   int4* nbr = nullptr;
+  int4* tiles = nullptr;     // tile runs
+  int* tile_items = nullptr;  // per-tile face lists
+  int* tile_count = nullptr;
+  int ntiles = 0;
   unsigned long long* err = nullptr;
   double2* aos = nullptr;
   double *W = nullptr, *partial = nullptr, *tot = nullptr;
@@ -242,7 +175,9 @@ void release(vt_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->rk4_graph) cudaGraphExecDestroy(c->rk4_graph);
-  void* bufs[] = {c->U, c->A, c->Sa, c->Sb, c->R, c->geo, c->nbr, c->err, c->aos, c->W, c->partial, c->tot};
+  void* bufs[] = {c->U,  c->A,     c->Sa,  c->Sb,         c->R,          c->geo,     c->nbr,
+                  c->err, c->aos,  c->W,   c->partial,    c->tot,        c->tiles,   c->tile_items,
+                  c->tile_count};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -258,6 +193,10 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
   a.out = out;
   a.geo = c->geo;
   a.nbr = c->nbr;
+  a.tiles = c->tiles;
+  a.tile_items = c->tile_items;
+  a.tile_count = c->tile_count;
+  a.ntiles = c->ntiles;
   a.err = c->err;
   a.Kpad = c->Kpad;
   a.K = c->K;
@@ -427,6 +366,30 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
     set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_create upload", e)));
     release(c);
     return nullptr;
+  }
+  // tile schedule: two-row tiles on the reference's structured mesh, runs of
+  // consecutive elements otherwise; then each tile's face list
+  {
+    const std::vector<int4> runs = vt::structured_tile_runs(K, d->element_type, d->neighbours);
+    c->ntiles = runs.empty() ? (K + vt::kTileElems - 1) / vt::kTileElems : static_cast<int>(runs.size());
+    if ((e = alloc(&c->tiles, sizeof(int4) * c->ntiles)) ||
+        (e = alloc(&c->tile_items, sizeof(int) * vt::kMaxItems * static_cast<size_t>(c->ntiles))) ||
+        (e = alloc(&c->tile_count, sizeof(int) * c->ntiles))) {
+      set(fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, vt::cuda_msg("tiles", e)));
+      release(c);
+      return nullptr;
+    }
+    if (runs.empty())
+      e = vt::launch_contiguous_tiles(c->tiles, K, c->ntiles, c->stream);
+    else
+      e = cudaMemcpyAsync(c->tiles, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = vt::launch_build_tile_items(c->tiles, c->nbr, c->tile_items, c->tile_count, c->ntiles, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    if (e) {
+      set(fail(VT_ERR_CUDA, vt::cuda_msg("tile schedule", e)));
+      release(c);
+      return nullptr;
+    }
   }
   set(VT_OK);
   return c;

@@ -1,22 +1,23 @@
 // The fused RK stage kernel, tiled through shared memory.
 //
-// A persistent block walks tiles of E consecutive elements and advances each
-// through one stage of the nodal DG scheme (Evolve.cpp:135-308,
-// numerical_flux Numericalflux.cpp:13-157, stage update Timestepping.cpp:85-306
-// / :39-82). The state crosses HBM once per stage:
+// A persistent block walks tiles of 64 elements (two runs of 32 consecutive
+// elements, see StageArgs) and advances each through one stage of the nodal
+// DG scheme (Evolve.cpp:135-308, numerical_flux Numericalflux.cpp:13-157,
+// stage update Timestepping.cpp:85-306 / :39-82). The state crosses HBM once
+// per stage:
 //
 //   0. prefetch (TMA bulk prefetch into L2) the next tile's state rows,
-//             geometry and neighbour table, and this tile's RK base and
+//             geometry and neighbour rows, and this tile's RK base and
 //             accumulator rows, so the dependent loads below hit L2;
-//   1. load   the tile's state (2*Np double2 rows x E), the neighbours across
-//             side 0 (their p+1 side nodes) and the neighbour table into
-//             shared memory;
-//   2. faces  one work item per (edge, Gauss point). An edge between two tile
-//             elements is evaluated once, by the element with the smaller
-//             index, and its flux is written to both elements' slots (the
-//             partner sees -F at the mirrored point nfq-1-q, its outward
-//             normal being -n); an edge leaving the tile is evaluated by each
-//             side, as in the reference;
+//   1. load   the tile's state (2*Np double2 rows), the neighbours across
+//             side 0 (their p+1 side nodes), the neighbour table and the
+//             tile's face list into shared memory;
+//   2. faces  one work item per (face, Gauss point) from the list built once
+//             at set-up (vt_schedule.cuh). A face between two tile elements
+//             is evaluated once, by the element with the smaller index, and
+//             written to both elements' slots (the partner sees -F at the
+//             mirrored point nfq-1-q, its outward normal being -n); a face
+//             leaving the tile is evaluated by each side, as in the reference;
 //   3. lift   4 threads per element, one conserved component each: surface
 //             term -(len_s/detJ) LIFT_s F_s into Np accumulators;
 //   4. flux   the nodal Euler flux of every node, contracted with the inverse
@@ -34,8 +35,9 @@ namespace vt {
 
 __host__ __device__ constexpr int align16(int b) { return (b + 15) / 16 * 16; }
 
-template <int P, int NFQ, int E>
+template <int P, int NFQ>
 struct TileLayout {
+  static constexpr int E = kTileElems;
   static constexpr int NP = np_of_p(P);
   static constexpr int NE = P + 1;
   static constexpr int ES = E + 1;  // padded row length (elements)
@@ -47,9 +49,9 @@ struct TileLayout {
   static constexpr int kTP = align16(kFB + kFBDoubles * 8);      // double [3][NFQ][NE]
   static constexpr int kTM = align16(kTP + 3 * NFQ * NE * 8);    // double [3][NFQ][NE]
   static constexpr int kNB = align16(kTM + 3 * NFQ * NE * 8);    // int4 [E]
-  static constexpr int kItems = align16(kNB + E * 16);           // int [3E]
-  static constexpr int kCount = align16(kItems + 3 * E * 4);     // int [32]
-  static constexpr int kBytes = align16(kCount + 32 * 4);
+  static constexpr int kEL = align16(kNB + E * 16);              // int [E] global element index
+  static constexpr int kItems = align16(kEL + E * 4);            // int [kMaxItems]
+  static constexpr int kBytes = align16(kItems + kMaxItems * 4);
 };
 
 // L2 prefetch of [p, p + bytes) through the TMA unit; bytes is a multiple of
@@ -58,45 +60,38 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <int NP, int E>
-__device__ __forceinline__ void prefetch_tile(const StageArgs& a, int tile, bool current, int t) {
-  const int e0 = tile * E;
-  const int ne = min(E, a.K - e0);
-  if (ne <= 0) return;
-  const unsigned bytes = static_cast<unsigned>(ne) * 16u;
+// Thread r (< 2 runs x rows) issues one row-run prefetch. `next`: the stage
+// input, geometry and neighbour rows of tile `run`; otherwise this tile's
+// accumulator and base rows (when the stage reads them).
+template <int NP>
+__device__ __forceinline__ void prefetch_runs(const StageArgs& a, const int4 run, bool next, int r) {
   const long long KP = a.Kpad;
-  int r = t;
-  if (!current) {
-    // the next tile: stage input rows, geometry rows, neighbour table
-    if (r < 2 * NP) {
-      prefetch_l2(a.in + r * KP + e0, bytes);
-      return;
-    }
-    r -= 2 * NP;
-    if (r < 7) {
-      prefetch_l2(a.geo + r * KP + e0, bytes);
-      return;
-    }
-    r -= 7;
-    if (r == 0) prefetch_l2(a.nbr + e0, bytes);
+  const int which = r & 1;
+  r >>= 1;
+  const int start = which ? run.z : run.x;
+  const int len = which ? run.w : run.y;
+  if (len <= 0) return;
+  const unsigned bytes = static_cast<unsigned>(len) * 16u;
+  if (next) {
+    if (r < 2 * NP) prefetch_l2(a.in + r * KP + start, bytes);
+    else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
+    else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
     return;
   }
-  // this tile: rows the stage update reads at the end
-  const bool want_base = a.stage == 1 || a.stage == 2;
-  const bool want_acc = a.stage >= 1 && a.stage <= 3;
   if (r < 2 * NP) {
-    if (want_acc) prefetch_l2(a.acc + r * KP + e0, bytes);
-    return;
+    if (a.stage >= 1 && a.stage <= 3) prefetch_l2(a.acc + r * KP + start, bytes);
+  } else if (r < 4 * NP) {
+    if (a.stage == 1 || a.stage == 2) prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
   }
-  r -= 2 * NP;
-  if (r < 2 * NP && want_base) prefetch_l2(a.base + r * KP + e0, bytes);
 }
 
-template <int P, int NFQ, int E>
+template <int P, int NFQ>
 // Three 256-thread blocks per SM (<= 80 registers per thread) keep 24 warps
-// resident alongside 3 x ~73 KB of shared memory.
-__global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a, const StageOps<P, NFQ> ops) {
-  using L = TileLayout<P, NFQ, E>;
+// resident alongside 3 x ~75 KB of shared memory.
+__global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const StageArgs a,
+                                                                        const StageOps<P, NFQ> ops) {
+  using L = TileLayout<P, NFQ>;
+  constexpr int E = L::E;
   constexpr int NP = L::NP;
   constexpr int NE = L::NE;
   constexpr int ES = L::ES;
@@ -108,12 +103,11 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
   double* TP = reinterpret_cast<double*>(smem + L::kTP);
   double* TM = reinterpret_cast<double*>(smem + L::kTM);
   int4* NB = reinterpret_cast<int4*>(smem + L::kNB);
+  int* EL = reinterpret_cast<int*>(smem + L::kEL);
   int* items = reinterpret_cast<int*>(smem + L::kItems);
-  int* counts = reinterpret_cast<int*>(smem + L::kCount);
 
   const int t = threadIdx.x;
   const long long KP = a.Kpad;
-  const int ntiles = (a.K + E - 1) / E;
 
   {
     const double* tp = &ops.tp[0][0][0];
@@ -124,63 +118,40 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
     }
   }
 
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int e0 = tile * E;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int4 run = __ldg(a.tiles + tile);
+    const int nitems = __ldg(a.tile_count + tile);
 
     // ---- 0. prefetch ------------------------------------------------------------
-    if (t < 32) {
-      if (tile + gridDim.x < ntiles) prefetch_tile<NP, E>(a, tile + gridDim.x, false, t);
-    } else if (t < 32 + 4 * NP) {
-      prefetch_tile<NP, E>(a, tile, true, t - 32);
+    if (t < 64) {
+      if (tile + gridDim.x < a.ntiles) prefetch_runs<NP>(a, __ldg(a.tiles + tile + gridDim.x), true, t);
+    } else if (t < 64 + 8 * NP) {
+      prefetch_runs<NP>(a, run, false, t - 64);
     }
 
     // ---- 1. load ------------------------------------------------------------------
     {
       const int col = t % E, grp = t / E;
-      const int e = e0 + col;
-      const bool valid = e < a.K;
-      int4 nb = make_int4(e, e, e, 0);
+      const int pos = col % kTileRun;
+      const bool second = col >= kTileRun;
+      const int e = (second ? run.z : run.x) + pos;
+      const bool valid = pos < (second ? run.w : run.y);
+      int4 nb = make_int4(0, 0, 0, 0);
       if (valid) nb = __ldg(a.nbr + e);
-      if (grp == 0) NB[col] = nb;
+      if (grp == 0) {
+        NB[col] = nb;
+        EL[col] = valid ? e : -1;
+      }
 #pragma unroll
       for (int r = grp; r < 2 * NP; r += 4)
         S[r * ES + col] = valid ? __ldg(a.in + r * KP + e) : make_double2(1.0, 0.0);
 #pragma unroll
       for (int r = grp; r < 2 * NE; r += 4)  // side 0 nodes are nodes 0..P: rows 0..2P+1
         H[r * ES + col] = valid ? __ldg(a.in + r * KP + nb.x) : make_double2(1.0, 0.0);
+      const int* src = a.tile_items + static_cast<long long>(tile) * kMaxItems;
+      for (int i = t; i < nitems; i += T) items[i] = __ldg(src + i);
     }
     __syncthreads();
-
-    // ---- edge list: (element, side) pairs this tile evaluates ----------------------
-    {
-      const int lane = t & 31, warp = t >> 5;
-      bool take = false;
-      int code = 0;
-      if (t < 3 * E) {
-        const int el = t / 3, s = t % 3;
-        if (e0 + el < a.K) {
-          const int4 nb4 = NB[el];
-          const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
-          const int nl = nb - e0;
-          const bool inside = nl >= 0 && nl < E;
-          take = !inside || (e0 + el < nb);
-          code = el | (s << 8) | ((inside && nb != e0 + el) ? (1 << 10) : 0);
-        }
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, take);
-      if (lane == 0) counts[warp] = __popc(m);
-      __syncthreads();
-      int base = 0;
-      for (int w = 0; w < warp; ++w) base += counts[w];
-      if (take) items[base + __popc(m & ((1u << lane) - 1u))] = code;
-      if (t == 0) {
-        int n = 0;
-        for (int w = 0; w < T / 32; ++w) n += counts[w];
-        counts[T / 32] = n;
-      }
-      __syncthreads();
-    }
-    const int nitems = counts[T / 32];
 
     // ---- 2. faces ----------------------------------------------------------------------
     for (int w = t; w < nitems * NFQ; w += T) {
@@ -188,11 +159,11 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
       const int q = w % NFQ;
       const int el = it & 0xff, s = (it >> 8) & 3;
       const bool mirror = (it >> 10) & 1;
-      const int e = e0 + el;
+      const int nl = (it >> 11) & 0xff;
+      const int e = EL[el];
+      const double2 n = __ldg(a.geo + (2 + s) * KP + e);
       const int4 nb4 = NB[el];
       const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
-      const int nl = nb - e0;
-      const bool inside = nl >= 0 && nl < E;
       double up[4] = {0, 0, 0, 0}, um[4] = {0, 0, 0, 0};
 #pragma unroll
       for (int k = 0; k < NE; ++k) {
@@ -201,7 +172,7 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
         const double cm = TM[(s * NFQ + q) * NE + k];
         const double2 o0 = S[(2 * node) * ES + el], o1 = S[(2 * node + 1) * ES + el];
         double2 n0, n1;
-        if (inside) {
+        if (mirror) {
           n0 = S[(2 * node) * ES + nl];
           n1 = S[(2 * node + 1) * ES + nl];
         } else if (s == 0) {
@@ -211,16 +182,15 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
           n0 = __ldg(a.in + (2 * node) * KP + nb);
           n1 = __ldg(a.in + (2 * node + 1) * KP + nb);
         }
-        up[0] += cp * o0.x;
-        up[1] += cp * o0.y;
-        up[2] += cp * o1.x;
-        up[3] += cp * o1.y;
-        um[0] += cm * n0.x;
-        um[1] += cm * n0.y;
-        um[2] += cm * n1.x;
-        um[3] += cm * n1.y;
+        up[0] = fma(cp, o0.x, up[0]);
+        up[1] = fma(cp, o0.y, up[1]);
+        up[2] = fma(cp, o1.x, up[2]);
+        up[3] = fma(cp, o1.y, up[3]);
+        um[0] = fma(cm, n0.x, um[0]);
+        um[1] = fma(cm, n0.y, um[1]);
+        um[2] = fma(cm, n1.x, um[2]);
+        um[3] = fma(cm, n1.y, um[3]);
       }
-      const double2 n = __ldg(a.geo + (2 + s) * KP + e);
       double f[4];
       const int code = roe_flux(up, um, n.x, n.y, f);
       if (code) record_error(a, NFQ, e, q, s, code);
@@ -236,9 +206,9 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
     // ---- 3. lift: thread (element el, component c) --------------------------------------
     const int c = t / E;  // uniform per warp
     const int el = t % E;
-    const int e = e0 + el;
-    const bool valid = e < a.K;
-    const int eg = valid ? e : e0;
+    const int e = EL[el];
+    const bool valid = e >= 0;
+    const int eg = valid ? e : run.x;
     double r[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) r[i] = 0.0;
@@ -252,7 +222,7 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
         for (int q = 0; q < NFQ; ++q) {
           const double fs = ls * FB[((s * 4 + c) * NFQ + q) * ES + el];
 #pragma unroll
-          for (int i = 0; i < NP; ++i) r[i] -= ops.lift[s][i][q] * fs;
+          for (int i = 0; i < NP; ++i) r[i] = fma(-ops.lift[s][i][q], fs, r[i]);
         }
       }
     }
@@ -282,7 +252,7 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
         const double gx = G[(j * 8 + c) * ES + el];
         const double gy = G[(j * 8 + 4 + c) * ES + el];
 #pragma unroll
-        for (int i = 0; i < NP; ++i) r[i] += ops.D[0][i][j] * gx + ops.D[1][i][j] * gy;
+        for (int i = 0; i < NP; ++i) r[i] = fma(ops.D[0][i][j], gx, fma(ops.D[1][i][j], gy, r[i]));
       }
     }
 
@@ -300,25 +270,25 @@ __global__ void __launch_bounds__(4 * E, 3) tile_stage_kernel(const StageArgs a,
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
             const double u = sv[i * 4 * ES];
-            acc[i * step] = u + a.c_acc * r[i];
-            out[i * step] = u + a.c_out * r[i];
+            acc[i * step] = fma(a.c_acc, r[i], u);
+            out[i * step] = fma(a.c_out, r[i], u);
           }
           break;
         case 1:
         case 2:
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
-            acc[i * step] = acc[i * step] + a.c_acc * r[i];
-            out[i * step] = __ldg(base + i * step) + a.c_out * r[i];
+            acc[i * step] = fma(a.c_acc, r[i], acc[i * step]);
+            out[i * step] = fma(a.c_out, r[i], __ldg(base + i * step));
           }
           break;
         case 3:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = acc[i * step] + a.c_out * r[i];
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(a.c_out, r[i], acc[i * step]);
           break;
         case kStageEuler:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = sv[i * 4 * ES] + a.c_out * r[i];
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(a.c_out, r[i], sv[i * 4 * ES]);
           break;
         default:
 #pragma unroll
