@@ -258,7 +258,8 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
   if (!e) e = cudaMemcpyAsync(words, errw, sizeof(words), cudaMemcpyDeviceToHost, st);
   if (!e) e = cudaStreamSynchronize(st);
   if (e) return fail(VT_ERR_CUDA, std::string("vt_step_rk4_noalloc: ") + cudaGetErrorString(e));
-  if (words[3]) return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: neighbour index out of range");
+  if (words[3] & 1ull) return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: neighbour index out of range");
+  if (words[3] & 2ull) return fail(VT_ERR_CUDA, "vt_step_rk4_noalloc: a bulk-copy wait gave up");
   if (words[0] == ~0ull) return VT_OK;
   const unsigned long long epoch = words[0] >> 40;
   unsigned long long local = words[0] & ((1ull << 40) - 1);

@@ -223,12 +223,15 @@ cudaError_t reset_error_words(vt_ctx* c) {
 
 // Waits for the stream, decodes the first-error key and advances the clock.
 int finish(vt_ctx* c, int nsteps, double dt) {
-  unsigned long long key = ~0ull;
-  cudaError_t e = cudaMemcpyAsync(&key, c->err, sizeof(key), cudaMemcpyDeviceToHost, c->stream);
+  unsigned long long words[4] = {~0ull, 0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(words, c->err, sizeof(words), cudaMemcpyDeviceToHost, c->stream);
   if (!e) e = cudaStreamSynchronize(c->stream);
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("step", e));
   for (int s = 0; s < nsteps; ++s) c->time += dt;  // Element::time += t_step per step
   c->last = vt_error_info{};
+  if (words[3] & 2ull)
+    return fail(VT_ERR_CUDA, "stage kernel: a bulk-copy wait gave up (the state is not valid)");
+  const unsigned long long key = words[0];
   if (key == ~0ull) return VT_OK;
   const unsigned long long epoch = key >> 40;
   unsigned long long local = key & ((1ull << 40) - 1);

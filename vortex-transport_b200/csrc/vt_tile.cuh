@@ -6,12 +6,11 @@
 // stage update Timestepping.cpp:85-306 / :39-82). The state crosses HBM once
 // per stage:
 //
-//   0. prefetch (TMA bulk prefetch into L2) the next tile's state rows,
-//             geometry and neighbour rows, and this tile's RK base and
-//             accumulator rows, so the dependent loads below hit L2;
-//   1. load   the tile's state (2*Np double2 rows), the neighbours across
-//             side 0 (their p+1 side nodes), the neighbour table and the
-//             tile's face list into shared memory;
+//   1. load   the tile's state rows arrive in shared memory by TMA bulk copies
+//             (cp.async.bulk, completion on an mbarrier) issued during the
+//             previous tile's volume phase; the side-0 neighbours' side nodes,
+//             the neighbour table and the tile's face list were loaded into
+//             registers during the previous tile as well;
 //   2. faces  one work item per (face, Gauss point) from the list built once
 //             at set-up (vt_schedule.cuh). A face between two tile elements
 //             is evaluated once, by the element with the smaller index, and
@@ -21,12 +20,18 @@
 //   3. lift   4 threads per element, one conserved component each: surface
 //             term -(len_s/detJ) LIFT_s F_s into Np accumulators;
 //   4. flux   the nodal Euler flux of every node, contracted with the inverse
-//             Jacobian, once, into shared memory;
+//             Jacobian, once, into shared memory; the state tile is then free
+//             and the next tile's copies are issued;
 //   5. volume D_xi G_xi + D_eta G_eta, then the RK stage update written back.
 //
+// Upcoming rows are also prefetched into L2 (cp.async.bulk.prefetch.L2) one
+// tile ahead and the tile's geometry rows into L1, so no phase waits on HBM.
 // The reference's mass-inverse apply is folded into D and LIFT on the host.
 // Shared-memory rows are padded by one element so that rows that differ by a
 // multiple of 128 bytes do not fall into the same banks.
+//
+// Every wait on the mbarrier is bounded; a wait that gives up sets bit 1 of
+// err[3], and the block stops taking tiles.
 #pragma once
 
 #include "vt_device.cuh"
@@ -51,37 +56,77 @@ struct TileLayout {
   static constexpr int kNB = align16(kTM + 3 * NFQ * NE * 8);    // int4 [E]
   static constexpr int kEL = align16(kNB + E * 16);              // int [E] global element index
   static constexpr int kItems = align16(kEL + E * 4);            // int [kMaxItems]
-  static constexpr int kBytes = align16(kItems + kMaxItems * 4);
+  static constexpr int kBar = align16(kItems + kMaxItems * 4);   // mbarrier (8 B) + abort flag
+  static constexpr int kBytes = align16(kBar + 16);
 };
 
-// L2 prefetch of [p, p + bytes) through the TMA unit; bytes is a multiple of
-// 16 and p is 16-byte aligned (every row start of the SoA layout is).
+// ---- TMA unit ------------------------------------------------------------------
+// L2 prefetch of [p, p + bytes) (bytes a multiple of 16, p 16-byte aligned).
 __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// Thread r (< 2 runs x rows) issues one row-run prefetch. `next`: the stage
-// input, geometry and neighbour rows of tile `run`; otherwise this tile's
-// accumulator and base rows (when the stage reads them).
-template <int NP>
-__device__ __forceinline__ void prefetch_runs(const StageArgs& a, const int4 run, bool next, int r) {
-  const long long KP = a.Kpad;
-  const int which = r & 1;
-  r >>= 1;
-  const int start = which ? run.z : run.x;
-  const int len = which ? run.w : run.y;
-  if (len <= 0) return;
-  const unsigned bytes = static_cast<unsigned>(len) * 16u;
-  if (next) {
-    if (r < 2 * NP) prefetch_l2(a.in + r * KP + start, bytes);
-    else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
-    else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
-    return;
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+// true once the phase with parity `parity` has completed.
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bulk copy of `bytes` (multiple of 16, both ends 16-byte aligned) from global
+// to this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr unsigned kMaxWaitTries = 1u << 22;
+
+// Warp 0 issues the bulk copies of a tile's 2*Np state rows (two runs each)
+// into S, after lane 0 announced the byte count on the barrier.
+template <int NP, int ES>
+__device__ __forceinline__ void issue_tile_copies(const StageArgs& a, const int4 run, double2* S,
+                                                  unsigned long long* bar, int lane) {
+  const unsigned b0 = static_cast<unsigned>(run.y) * 16u, b1 = static_cast<unsigned>(run.w) * 16u;
+  if (lane == 0) {
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, 2u * NP * (b0 + b1));
   }
-  if (r < 2 * NP) {
-    if (a.stage >= 1 && a.stage <= 3) prefetch_l2(a.acc + r * KP + start, bytes);
-  } else if (r < 4 * NP) {
-    if (a.stage == 1 || a.stage == 2) prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
+  __syncwarp();
+  for (int l = lane; l < 4 * NP; l += 32) {
+    const int r = l >> 1, which = l & 1;
+    const int start = which ? run.z : run.x;
+    const unsigned bytes = which ? b1 : b0;
+    if (bytes) bulk_g2s(S + r * ES + which * kTileRun, a.in + r * a.Kpad + start, bytes, bar);
   }
 }
 
@@ -105,9 +150,14 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   int4* NB = reinterpret_cast<int4*>(smem + L::kNB);
   int* EL = reinterpret_cast<int*>(smem + L::kEL);
   int* items = reinterpret_cast<int*>(smem + L::kItems);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + L::kBar);
+  int* abort_flag = reinterpret_cast<int*>(smem + L::kBar + 8);
 
   const int t = threadIdx.x;
+  const int col = t % E, grp = t / E;  // load mapping; also (element, component) later
+  const int lane = t & 31;
   const long long KP = a.Kpad;
+  const int G = gridDim.x;
 
   {
     const double* tp = &ops.tp[0][0][0];
@@ -117,41 +167,98 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       TM[l] = tm[l];
     }
   }
+  if (t == 0) {
+    mbar_init(bar, 1);
+    *abort_flag = 0;
+  }
+  __syncthreads();
 
-  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-    const int4 run = __ldg(a.tiles + tile);
-    const int nitems = __ldg(a.tile_count + tile);
+  // tile metadata of the tile in hand: run, face count, this thread's face
+  // item, this column's neighbours and side-0 neighbour rows
+  int tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  int4 run = __ldg(a.tiles + tile);
+  int nitems = __ldg(a.tile_count + tile);
+  int my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
+  int4 my_nb = make_int4(0, 0, 0, 0);
+  double2 hreg[2];
+  {
+    const int pos = col % kTileRun;
+    const bool second = col >= kTileRun;
+    const bool valid = pos < (second ? run.w : run.y);
+    if (valid) my_nb = __ldg(a.nbr + (second ? run.z : run.x) + pos);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int r = grp + 4 * k;
+      hreg[k] = (valid && r < 2 * NE) ? __ldg(a.in + r * KP + my_nb.x) : make_double2(1.0, 0.0);
+    }
+  }
+  if (t < 32) issue_tile_copies<NP, ES>(a, run, S, bar, lane);
+  unsigned parity = 0;
 
-    // ---- 0. prefetch ------------------------------------------------------------
+  for (; tile < a.ntiles; tile += G) {
+    const bool has_next = tile + G < a.ntiles;
+
+    // ---- prefetch: the tile after next into L2, this tile's RK rows ----------------
     if (t < 64) {
-      if (tile + gridDim.x < a.ntiles) prefetch_runs<NP>(a, __ldg(a.tiles + tile + gridDim.x), true, t);
+      if (tile + 2 * G < a.ntiles) {
+        const int4 rr = __ldg(a.tiles + tile + 2 * G);
+        const int which = t & 1, r = t >> 1;
+        const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
+        if (len > 0) {
+          const unsigned bytes = static_cast<unsigned>(len) * 16u;
+          if (r < 2 * NP) prefetch_l2(a.in + r * KP + start, bytes);
+          else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
+          else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
+        }
+      }
     } else if (t < 64 + 8 * NP) {
-      prefetch_runs<NP>(a, run, false, t - 64);
+      const int l = t - 64, which = l & 1, r = l >> 1;
+      const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+      if (len > 0) {
+        const unsigned bytes = static_cast<unsigned>(len) * 16u;
+        if (r < 2 * NP) {
+          if (a.stage >= 1 && a.stage <= 3) prefetch_l2(a.acc + r * KP + start, bytes);
+        } else if (a.stage == 1 || a.stage == 2) {
+          prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
+        }
+      }
+    } else if (t < 64 + 8 * NP + 56) {
+      // this tile's 7 geometry rows into L1 (4 lines per 32-element run)
+      const int l = t - 64 - 8 * NP, row = l >> 3, which = (l >> 2) & 1, line = l & 3;
+      const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+      if (line * 8 < len) prefetch_l1(a.geo + row * KP + start + line * 8);
     }
 
     // ---- 1. load ------------------------------------------------------------------
+    int4 next_run = make_int4(0, 0, 0, 0);
+    if (has_next) next_run = __ldg(a.tiles + tile + G);
     {
-      const int col = t % E, grp = t / E;
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
-      const int e = (second ? run.z : run.x) + pos;
       const bool valid = pos < (second ? run.w : run.y);
-      int4 nb = make_int4(0, 0, 0, 0);
-      if (valid) nb = __ldg(a.nbr + e);
       if (grp == 0) {
-        NB[col] = nb;
-        EL[col] = valid ? e : -1;
+        NB[col] = my_nb;
+        EL[col] = valid ? (second ? run.z : run.x) + pos : -1;
       }
 #pragma unroll
-      for (int r = grp; r < 2 * NP; r += 4)
-        S[r * ES + col] = valid ? __ldg(a.in + r * KP + e) : make_double2(1.0, 0.0);
-#pragma unroll
-      for (int r = grp; r < 2 * NE; r += 4)  // side 0 nodes are nodes 0..P: rows 0..2P+1
-        H[r * ES + col] = valid ? __ldg(a.in + r * KP + nb.x) : make_double2(1.0, 0.0);
-      const int* src = a.tile_items + static_cast<long long>(tile) * kMaxItems;
-      for (int i = t; i < nitems; i += T) items[i] = __ldg(src + i);
+      for (int k = 0; k < 2; ++k) {
+        const int r = grp + 4 * k;
+        if (r < 2 * NE) H[r * ES + col] = hreg[k];
+      }
+      if (t < nitems) items[t] = my_item;
     }
+    {
+      bool ok = false;
+      for (unsigned n = 0; n < kMaxWaitTries && !ok; ++n) ok = mbar_try_wait(bar, parity);
+      if (!ok) {
+        atomicOr(&a.err[3], 2ull);
+        *abort_flag = 1;
+      }
+    }
+    parity ^= 1u;
     __syncthreads();
+    if (*abort_flag) break;
 
     // ---- 2. faces ----------------------------------------------------------------------
     for (int w = t; w < nitems * NFQ; w += T) {
@@ -203,9 +310,19 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     }
     __syncthreads();
 
+    // next tile's metadata (next_run has arrived by now)
+    if (has_next) {
+      nitems = __ldg(a.tile_count + tile + G);
+      my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
+      const int pos = col % kTileRun;
+      const bool second = col >= kTileRun;
+      my_nb = pos < (second ? next_run.w : next_run.y) ? __ldg(a.nbr + (second ? next_run.z : next_run.x) + pos)
+                                                       : make_int4(0, 0, 0, 0);
+    }
+
     // ---- 3. lift: thread (element el, component c) --------------------------------------
-    const int c = t / E;  // uniform per warp
-    const int el = t % E;
+    const int c = grp;  // uniform per warp
+    const int el = col;
     const int e = EL[el];
     const bool valid = e >= 0;
     const int eg = valid ? e : run.x;
@@ -229,8 +346,8 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     __syncthreads();
 
     // ---- 4. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ---------------
+    double* Gs = FB;
     if (P > 0) {
-      double* G = FB;
       const double2 j0 = __ldg(a.geo + 0 * KP + eg);
       const double2 j1 = __ldg(a.geo + 1 * KP + eg);
       for (int j = c; j < NP; j += 4) {
@@ -240,17 +357,32 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
         contravariant_flux(sv, j0.x, j0.y, j1.x, j1.y, gxi, geta);
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
-          G[(j * 8 + cc) * ES + el] = gxi[cc];
-          G[(j * 8 + 4 + cc) * ES + el] = geta[cc];
+          Gs[(j * 8 + cc) * ES + el] = gxi[cc];
+          Gs[(j * 8 + 4 + cc) * ES + el] = geta[cc];
         }
       }
-      __syncthreads();
+    }
+    __syncthreads();
 
-      // ---- 5a. volume ------------------------------------------------------------------
+    // the state tile is free: start the next tile's copies and neighbour rows
+    if (has_next) {
+      if (t < 32) issue_tile_copies<NP, ES>(a, next_run, S, bar, lane);
+      const int pos = col % kTileRun;
+      const bool second = col >= kTileRun;
+      const bool nvalid = pos < (second ? next_run.w : next_run.y);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int rr = grp + 4 * k;
+        hreg[k] = (nvalid && rr < 2 * NE) ? __ldg(a.in + rr * KP + my_nb.x) : make_double2(1.0, 0.0);
+      }
+    }
+
+    // ---- 5a. volume ------------------------------------------------------------------
+    if (P > 0) {
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
-        const double gx = G[(j * 8 + c) * ES + el];
-        const double gy = G[(j * 8 + 4 + c) * ES + el];
+        const double gx = Gs[(j * 8 + c) * ES + el];
+        const double gy = Gs[(j * 8 + 4 + c) * ES + el];
 #pragma unroll
         for (int i = 0; i < NP; ++i) r[i] = fma(ops.D[0][i][j], gx, fma(ops.D[1][i][j], gy, r[i]));
       }
@@ -260,16 +392,16 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     if (valid) {
       const int h = c >> 1, part = c & 1;
       const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
+      const double* in = reinterpret_cast<const double*>(a.in) + off0;
       const double* base = reinterpret_cast<const double*>(a.base) + off0;
       double* acc = reinterpret_cast<double*>(a.acc) + off0;
       double* out = reinterpret_cast<double*>(a.out) + off0;
-      const double* sv = reinterpret_cast<const double*>(S + h * ES + el) + part;
       const long long step = 4 * KP;  // doubles between node rows of the same pair
       switch (a.stage) {
         case 0:
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
-            const double u = sv[i * 4 * ES];
+            const double u = __ldg(in + i * step);
             acc[i * step] = fma(a.c_acc, r[i], u);
             out[i * step] = fma(a.c_out, r[i], u);
           }
@@ -288,7 +420,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
           break;
         case kStageEuler:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = fma(a.c_out, r[i], sv[i * 4 * ES]);
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(a.c_out, r[i], __ldg(in + i * step));
           break;
         default:
 #pragma unroll
@@ -296,9 +428,16 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
           break;
       }
     }
+    run = next_run;
     __syncthreads();  // the next tile reuses the shared buffers
   }
 
+  if (*abort_flag) {
+    // the bulk copies of a tile whose wait gave up may still land: wait for
+    // them once more, with the same bound, before the block leaves
+    for (unsigned n = 0; n < kMaxWaitTries; ++n)
+      if (mbar_try_wait(bar, parity ^ 1u)) break;
+  }
   if (a.stage == 3 || a.stage == kStageEuler) {
     if (t == 0) {
       __threadfence();
