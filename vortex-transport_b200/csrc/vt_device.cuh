@@ -95,16 +95,21 @@ __device__ __forceinline__ void record_error(const StageArgs& a, int nfq, int e,
 }
 
 // Roe flux with the reference's entropy fix and its squared "sound speed"
-// ci = c2^2 (Numericalflux.cpp:13-157), rearranged to need two reciprocals, one
-// square root and two further reciprocals per call:
+// ci = c2^2 (Numericalflux.cpp:13-157), rearranged to need one reciprocal for
+// both densities, one square root and two further reciprocals per call:
 //   p = (gamma-1) (rhoE - (m_x u + m_y v) / 2) with u = m_x / rho,
-//   sqrt(rhoR / rhoL) = sqrt(rhoR * (1 / rhoL)), 1 / eps = 10 / ci.
+//   1/rhoL = rhoR / (rhoL rhoR), sqrt(rhoR / rhoL) = sqrt(rhoR * (1 / rhoL)),
+//   1 / eps = 10 / ci.
 // Equal to the reference's expression up to rounding. Returns the reference's
 // error code (1 left state, 2 right state, 3 c2 <= 0) or 0.
 __device__ __forceinline__ int roe_flux(const double* uL, const double* uR, double nx, double ny,
                                         double* f) {
   const double rL = uL[0];
-  const double irL = 1.0 / rL;
+  const double rR = uR[0];
+  // one reciprocal serves both densities: 1/rL = rR / (rL rR), 1/rR = rL / (rL rR)
+  const double irLR = 1.0 / (rL * rR);
+  const double irL = rR * irLR;
+  const double irR = rL * irLR;
   const double vxL = uL[1] * irL, vyL = uL[2] * irL;
   const double unL = vxL * nx + vyL * ny;
   const double pL = kGm1 * (uL[3] - 0.5 * (uL[1] * vxL + uL[2] * vyL));
@@ -113,8 +118,6 @@ __device__ __forceinline__ int roe_flux(const double* uL, const double* uR, doub
   const double rHL = uL[3] + pL;
   const double HL = rHL * irL;
 
-  const double rR = uR[0];
-  const double irR = 1.0 / rR;
   const double vxR = uR[1] * irR, vyR = uR[2] * irR;
   const double unR = vxR * nx + vyR * ny;
   const double pR = kGm1 * (uR[3] - 0.5 * (uR[1] * vxR + uR[2] * vyR));

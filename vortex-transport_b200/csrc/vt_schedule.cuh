@@ -52,14 +52,17 @@ __global__ void contiguous_tiles_kernel(int4* tiles, int K, int ntiles) {
 
 // One block of 256 threads per tile: every (element, side) of the tile is a
 // candidate; it is evaluated here when the neighbour is outside the tile or
-// has a larger index. Written in (element, side) order.
+// has a larger index. Grouped by how the outer state is found -- a partner in
+// the tile, a side-0 neighbour staged in shared memory, any other neighbour
+// read from global memory -- so that a warp's work items take one path, and
+// in (element, side) order within a group.
 __global__ void build_tile_items_kernel(const int4* __restrict__ tiles, const int4* __restrict__ nbr,
                                         int* __restrict__ items, int* __restrict__ count) {
-  __shared__ int warp_n[8];
+  __shared__ int warp_n[3][8];
   const int tile = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int4 run = tiles[tile];
   bool take = false;
-  int code = 0;
+  int code = 0, cls = 0;
   if (t < kMaxItems) {
     const int el = t / 3, s = t % 3;
     const int pos = el % kTileRun;
@@ -74,17 +77,25 @@ __global__ void build_tile_items_kernel(const int4* __restrict__ tiles, const in
       const bool inside = nl >= 0 && nb != e;
       take = !inside || e < nb;
       code = el | (s << 8) | (inside ? (1 << 10) | (nl << 11) : 0);
+      cls = inside ? 0 : (s == 0 ? 1 : 2);
     }
   }
-  const unsigned m = __ballot_sync(0xffffffffu, take);
-  if (lane == 0) warp_n[warp] = __popc(m);
+  unsigned m[3];
+  for (int k = 0; k < 3; ++k) {
+    m[k] = __ballot_sync(0xffffffffu, take && cls == k);
+    if (lane == 0) warp_n[k][warp] = __popc(m[k]);
+  }
   __syncthreads();
   int base = 0;
-  for (int w = 0; w < warp; ++w) base += warp_n[w];
-  if (take) items[static_cast<long long>(tile) * kMaxItems + base + __popc(m & ((1u << lane) - 1u))] = code;
+  for (int k = 0; k < cls; ++k)
+    for (int w = 0; w < 8; ++w) base += warp_n[k][w];
+  for (int w = 0; w < warp; ++w) base += warp_n[cls][w];
+  if (take)
+    items[static_cast<long long>(tile) * kMaxItems + base + __popc(m[cls] & ((1u << lane) - 1u))] = code;
   if (t == 0) {
     int n = 0;
-    for (int w = 0; w < 8; ++w) n += warp_n[w];
+    for (int k = 0; k < 3; ++k)
+      for (int w = 0; w < 8; ++w) n += warp_n[k][w];
     count[tile] = n;
   }
 }

@@ -11,18 +11,23 @@
 //             previous tile's volume phase; the side-0 neighbours' side nodes,
 //             the neighbour table and the tile's face list were loaded into
 //             registers during the previous tile as well;
-//   2. faces  one work item per (face, Gauss point) from the list built once
-//             at set-up (vt_schedule.cuh). A face between two tile elements
-//             is evaluated once, by the element with the smaller index, and
-//             written to both elements' slots (the partner sees -F at the
-//             mirrored point nfq-1-q, its outward normal being -n); a face
-//             leaving the tile is evaluated by each side, as in the reference;
-//   3. lift   4 threads per element, one conserved component each: surface
+//   2. traces 4 threads per element, one conserved component each, evaluate
+//             the element's own trace at every face point from the p+1 side
+//             nodes (coefficients are immediates);
+//   3. faces  one work item per (face, Gauss point) from the list built once
+//             at set-up (vt_schedule.cuh), sorted so warps stay on one path.
+//             A face between two tile elements is evaluated once, by the
+//             element with the smaller index: its outer state is the partner's
+//             own trace at the mirrored point nfq-1-q, and the flux is written
+//             over both traces (the partner gets -F, its outward normal being
+//             -n). A face leaving the tile is evaluated by each side, as in
+//             the reference, with the outer trace from the neighbour's nodes;
+//   4. lift   4 threads per element, one conserved component each: surface
 //             term -(len_s/detJ) LIFT_s F_s into Np accumulators;
-//   4. flux   the nodal Euler flux of every node, contracted with the inverse
+//   5. flux   the nodal Euler flux of every node, contracted with the inverse
 //             Jacobian, once, into shared memory; the state tile is then free
 //             and the next tile's copies are issued;
-//   5. volume D_xi G_xi + D_eta G_eta, then the RK stage update written back.
+//   6. volume D_xi G_xi + D_eta G_eta, then the RK stage update written back.
 //
 // Upcoming rows are also prefetched into L2 (cp.async.bulk.prefetch.L2) one
 // tile ahead and the tile's geometry rows into L1, so no phase waits on HBM.
@@ -51,8 +56,7 @@ struct TileLayout {
   static constexpr int kS = 0;                                   // double2 [2NP][ES]
   static constexpr int kH = align16(kS + 2 * NP * ES * 16);      // double2 [2NE][ES]
   static constexpr int kFB = align16(kH + 2 * NE * ES * 16);     // double [3][4][NFQ][ES] | [NP][8][ES]
-  static constexpr int kTP = align16(kFB + kFBDoubles * 8);      // double [3][NFQ][NE]
-  static constexpr int kTM = align16(kTP + 3 * NFQ * NE * 8);    // double [3][NFQ][NE]
+  static constexpr int kTM = align16(kFB + kFBDoubles * 8);      // double [3][NFQ][NE]
   static constexpr int kNB = align16(kTM + 3 * NFQ * NE * 8);    // int4 [E]
   static constexpr int kEL = align16(kNB + E * 16);              // int [E] global element index
   static constexpr int kItems = align16(kEL + E * 4);            // int [kMaxItems]
@@ -145,7 +149,6 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   double2* S = reinterpret_cast<double2*>(smem + L::kS);
   double2* H = reinterpret_cast<double2*>(smem + L::kH);
   double* FB = reinterpret_cast<double*>(smem + L::kFB);
-  double* TP = reinterpret_cast<double*>(smem + L::kTP);
   double* TM = reinterpret_cast<double*>(smem + L::kTM);
   int4* NB = reinterpret_cast<int4*>(smem + L::kNB);
   int* EL = reinterpret_cast<int*>(smem + L::kEL);
@@ -160,12 +163,8 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   const int G = gridDim.x;
 
   {
-    const double* tp = &ops.tp[0][0][0];
     const double* tm = &ops.tm[0][0][0];
-    for (int l = t; l < 3 * NFQ * NE; l += T) {
-      TP[l] = tp[l];
-      TM[l] = tm[l];
-    }
+    for (int l = t; l < 3 * NFQ * NE; l += T) TM[l] = tm[l];
   }
   if (t == 0) {
     mbar_init(bar, 1);
@@ -199,10 +198,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   for (; tile < a.ntiles; tile += G) {
     const bool has_next = tile + G < a.ntiles;
 
-    // ---- prefetch: the tile after next into L2, this tile's RK rows ----------------
+    // ---- prefetch: the next tile into L2 (its state copies start in phase 5), this
+    // tile's RK rows into L2 and its geometry rows into L1 -----------------------
     if (t < 64) {
-      if (tile + 2 * G < a.ntiles) {
-        const int4 rr = __ldg(a.tiles + tile + 2 * G);
+      if (has_next) {
+        const int4 rr = __ldg(a.tiles + tile + G);
         const int which = t & 1, r = t >> 1;
         const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
         if (len > 0) {
@@ -260,43 +260,63 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     __syncthreads();
     if (*abort_flag) break;
 
-    // ---- 2. faces ----------------------------------------------------------------------
+    // ---- 2. own traces: Tr[s][c][q][el], thread (element el, component c) ----------
+    {
+      const int cc = grp, el = col;
+      const double* Sd = reinterpret_cast<const double*>(S);
+      double u[NP];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) u[i] = Sd[((2 * i + (cc >> 1)) * ES + el) * 2 + (cc & 1)];
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+#pragma unroll
+        for (int q = 0; q < NFQ; ++q) {
+          double v = 0.0;
+#pragma unroll
+          for (int k = 0; k < NE; ++k) v = fma(ops.tp[s][q][k], u[edge_node(P, s, k)], v);
+          FB[((s * 4 + cc) * NFQ + q) * ES + el] = v;
+        }
+    }
+    __syncthreads();
+
+    // ---- 3. faces: the flux overwrites the traces it consumed ----------------------------
     for (int w = t; w < nitems * NFQ; w += T) {
       const int it = items[w / NFQ];
       const int q = w % NFQ;
       const int el = it & 0xff, s = (it >> 8) & 3;
       const bool mirror = (it >> 10) & 1;
       const int nl = (it >> 11) & 0xff;
+      const int qm = NFQ - 1 - q;
       const int e = EL[el];
       const double2 n = __ldg(a.geo + (2 + s) * KP + e);
-      const int4 nb4 = NB[el];
-      const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
-      double up[4] = {0, 0, 0, 0}, um[4] = {0, 0, 0, 0};
+      double up[4], um[4];
 #pragma unroll
-      for (int k = 0; k < NE; ++k) {
-        const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
-        const double cp = TP[(s * NFQ + q) * NE + k];
-        const double cm = TM[(s * NFQ + q) * NE + k];
-        const double2 o0 = S[(2 * node) * ES + el], o1 = S[(2 * node + 1) * ES + el];
-        double2 n0, n1;
-        if (mirror) {
-          n0 = S[(2 * node) * ES + nl];
-          n1 = S[(2 * node + 1) * ES + nl];
-        } else if (s == 0) {
-          n0 = H[(2 * k) * ES + el];
-          n1 = H[(2 * k + 1) * ES + el];
-        } else {
-          n0 = __ldg(a.in + (2 * node) * KP + nb);
-          n1 = __ldg(a.in + (2 * node + 1) * KP + nb);
+      for (int c = 0; c < 4; ++c) up[c] = FB[((s * 4 + c) * NFQ + q) * ES + el];
+      if (mirror) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) um[c] = FB[((s * 4 + c) * NFQ + qm) * ES + nl];
+      } else {
+        const int4 nb4 = NB[el];
+        const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) um[c] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NE; ++k) {
+          const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
+          const double cm = TM[(s * NFQ + q) * NE + k];
+          double2 n0, n1;
+          if (s == 0) {
+            n0 = H[(2 * k) * ES + el];
+            n1 = H[(2 * k + 1) * ES + el];
+          } else {
+            n0 = __ldg(a.in + (2 * node) * KP + nb);
+            n1 = __ldg(a.in + (2 * node + 1) * KP + nb);
+          }
+          um[0] = fma(cm, n0.x, um[0]);
+          um[1] = fma(cm, n0.y, um[1]);
+          um[2] = fma(cm, n1.x, um[2]);
+          um[3] = fma(cm, n1.y, um[3]);
         }
-        up[0] = fma(cp, o0.x, up[0]);
-        up[1] = fma(cp, o0.y, up[1]);
-        up[2] = fma(cp, o1.x, up[2]);
-        up[3] = fma(cp, o1.y, up[3]);
-        um[0] = fma(cm, n0.x, um[0]);
-        um[1] = fma(cm, n0.y, um[1]);
-        um[2] = fma(cm, n1.x, um[2]);
-        um[3] = fma(cm, n1.y, um[3]);
       }
       double f[4];
       const int code = roe_flux(up, um, n.x, n.y, f);
@@ -305,7 +325,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + q) * ES + el] = f[c];
       if (mirror) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + (NFQ - 1 - q)) * ES + nl] = -f[c];
+        for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + qm) * ES + nl] = -f[c];
       }
     }
     __syncthreads();
@@ -320,7 +340,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
                                                        : make_int4(0, 0, 0, 0);
     }
 
-    // ---- 3. lift: thread (element el, component c) --------------------------------------
+    // ---- 4. lift: thread (element el, component c) --------------------------------------
     const int c = grp;  // uniform per warp
     const int el = col;
     const int e = EL[el];
@@ -345,7 +365,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     }
     __syncthreads();
 
-    // ---- 4. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ---------------
+    // ---- 5. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ---------------
     double* Gs = FB;
     if (P > 0) {
       const double2 j0 = __ldg(a.geo + 0 * KP + eg);
@@ -377,7 +397,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       }
     }
 
-    // ---- 5a. volume ------------------------------------------------------------------
+    // ---- 6a. volume ------------------------------------------------------------------
     if (P > 0) {
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
@@ -388,7 +408,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       }
     }
 
-    // ---- 5b. stage update: component c of every node ----------------------------------
+    // ---- 6b. stage update: component c of every node ----------------------------------
     if (valid) {
       const int h = c >> 1, part = c & 1;
       const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
