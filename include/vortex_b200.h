@@ -188,6 +188,38 @@ void* vt_stream(vt_ctx* ctx);
  * `reps` steps of size dt. Advances the state by `reps` steps. */
 int vt_profile_rk4_stages(vt_ctx* ctx, double dt, int reps, float* ms);
 
+/* ---- batched ensemble --------------------------------------------------- */
+/* Many independent problems (meshes of any size, p = 0..3) advanced together:
+ * the reference runs one problem per process (main.cpp:81-197), so this is
+ * `n` calls of rk4 (Timestepping.cpp:85-306) sharing each kernel launch.
+ * Instances with the same p and reference tables form a group stored as one
+ * ragged element array; one stage launch per group advances all its
+ * instances, and one CUDA graph holds a whole RK4 step. Each instance keeps
+ * its own time step, and its elements see exactly the arithmetic of a
+ * vt_ctx built from the same descriptor. */
+typedef struct vt_batch vt_batch;
+
+vt_batch* vt_batch_create(const vt_mesh_desc* descs, int n, int device, int* status);
+void vt_batch_destroy(vt_batch* batch);
+int vt_batch_size(const vt_batch* batch);
+int vt_batch_groups(const vt_batch* batch);
+int vt_batch_group_info(const vt_batch* batch, int group, int* p, int* n_instances, int64_t* n_elements);
+/* Per-instance state transfer, host arrays in the reference layout. */
+int vt_batch_upload_state(vt_batch* batch, int instance, const double* U);
+int vt_batch_download_state(vt_batch* batch, int instance, double* U, double* F);
+/* Per-instance time steps, dt[n]. */
+int vt_batch_set_dt(vt_batch* batch, const double* dt);
+/* nsteps RK4 steps of every instance; blocks until done. A non-physical state
+ * returns its code; vt_batch_last_error names the instance. */
+int vt_batch_step_rk4(vt_batch* batch, int nsteps);
+int vt_batch_last_error(const vt_batch* batch, int* instance, vt_error_info* out);
+/* Times each group's RK4 step with 1..max resident blocks per SM (`trials`
+ * repetitions each), keeps the fastest and reports it per group in
+ * blocks_per_sm[groups]; the state is left unchanged. */
+int vt_batch_autotune(vt_batch* batch, int trials, int* blocks_per_sm);
+/* Applies a stored tuning (as reported by vt_batch_autotune). */
+int vt_batch_set_blocks_per_sm(vt_batch* batch, const int* blocks_per_sm);
+
 /* ---- stepping without device allocation --------------------------------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc:
  * code running while a host framework's pool or arena owns all device memory,

@@ -140,6 +140,22 @@ _SIGNATURES = {
     "vt_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "vt_profile_rk4_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_float)]),
+    "vt_batch_create": (ctypes.c_void_p, [ctypes.POINTER(vt_mesh_desc), ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "vt_batch_destroy": (None, [ctypes.c_void_p]),
+    "vt_batch_size": (ctypes.c_int, [ctypes.c_void_p]),
+    "vt_batch_groups": (ctypes.c_int, [ctypes.c_void_p]),
+    "vt_batch_group_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+    "vt_batch_upload_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "vt_batch_download_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                               ctypes.c_void_p]),
+    "vt_batch_set_dt": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "vt_batch_step_rk4": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "vt_batch_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(vt_error_info)]),
+    "vt_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "vt_batch_set_blocks_per_sm": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "vt_noalloc_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     "vt_step_rk4_noalloc": (ctypes.c_int, [ctypes.POINTER(vt_device_mesh), ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
@@ -434,6 +450,112 @@ class Solver:
     def close(self):
         if getattr(self, "_h", None):
             lib().vt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# batched ensemble
+# ---------------------------------------------------------------------------
+class Batch:
+    """Independent problems advanced together (vt_batch_* in the C ABI)."""
+
+    def __init__(self, problems, device: int = 0):
+        self._problems = list(problems)
+        n = len(self._problems)
+        descs = (vt_mesh_desc * n)()
+        for i, pb in enumerate(self._problems):
+            descs[i] = pb.mesh_desc()
+        st = ctypes.c_int(0)
+        self._h = lib().vt_batch_create(descs, n, device, ctypes.byref(st))
+        if not self._h:
+            raise VortexError(st.value, _message())
+        self.n = n
+        self.device = device
+        self.shapes = [(pb.K, pb.Np) for pb in self._problems]
+        for i, pb in enumerate(self._problems):
+            self.upload(i, pb.array("U0"))
+
+    @property
+    def groups(self) -> list[tuple[int, int, int]]:
+        """(p, instances, elements) per group."""
+        out = []
+        for g in range(lib().vt_batch_groups(self._h)):
+            p, ni, ne = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+            _check(lib().vt_batch_group_info(self._h, g, ctypes.byref(p), ctypes.byref(ni),
+                                             ctypes.byref(ne)))
+            out.append((p.value, ni.value, ne.value))
+        return out
+
+    def upload(self, i: int, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.shape == (*self.shapes[i], 4)
+        _check(lib().vt_batch_upload_state(self._h, i, U.ctypes.data_as(ctypes.c_void_p)))
+
+    def download(self, i: int) -> np.ndarray:
+        U = np.empty((*self.shapes[i], 4))
+        _check(lib().vt_batch_download_state(self._h, i, U.ctypes.data_as(ctypes.c_void_p), None))
+        return U
+
+    def set_dt(self, dt) -> None:
+        dt = np.ascontiguousarray(dt, dtype=np.float64)
+        assert dt.shape == (self.n,)
+        _check(lib().vt_batch_set_dt(self._h, _ptr(dt)))
+
+    def rk4(self, nsteps: int) -> None:
+        st = lib().vt_batch_step_rk4(self._h, int(nsteps))
+        if st in (VT_ERR_NONPHYSICAL_LEFT, VT_ERR_NONPHYSICAL_RIGHT, VT_ERR_NONPHYSICAL_C2):
+            info, inst = vt_error_info(), ctypes.c_int(-1)
+            lib().vt_batch_last_error(self._h, ctypes.byref(inst), ctypes.byref(info))
+            err = NonPhysicalState(st, _message(), info)
+            err.instance = inst.value
+            raise err
+        _check(st)
+
+    def autotune(self, trials: int = 3, cache: str | None = None) -> list[int]:
+        """Resident blocks per SM for each group, tuned on the device and cached
+        in `cache` (a JSON file keyed by the batch's makeup and the GPU)."""
+        import hashlib
+        import json
+        key = None
+        if cache:
+            import torch
+            props = torch.cuda.get_device_properties(self.device)
+            sig = json.dumps([self.groups, props.name, props.multi_processor_count])
+            key = hashlib.sha1(sig.encode()).hexdigest()
+            try:
+                with open(cache) as f:
+                    stored = json.load(f).get(key)
+            except (OSError, ValueError):
+                stored = None
+            if stored:
+                arr = (ctypes.c_int * len(stored))(*stored)
+                _check(lib().vt_batch_set_blocks_per_sm(self._h, arr))
+                return list(stored)
+        ng = lib().vt_batch_groups(self._h)
+        arr = (ctypes.c_int * ng)()
+        _check(lib().vt_batch_autotune(self._h, int(trials), arr))
+        best = list(arr)
+        if cache:
+            try:
+                with open(cache) as f:
+                    data = json.load(f)
+            except (OSError, ValueError):
+                data = {}
+            data[key] = best
+            os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+            with open(cache, "w") as f:
+                json.dump(data, f, indent=1)
+        return best
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vt_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

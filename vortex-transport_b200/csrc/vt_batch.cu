@@ -1,0 +1,571 @@
+// Batched ensemble: many independent vortex problems advanced together
+// (vt_batch_* in include/vortex_b200.h). The reference runs one problem per
+// process; this has no reference counterpart beyond the per-problem stepper.
+//
+// Instances with the same polynomial order and the same reference operators
+// (p, line rule, mass/stiffness tables) form a group. A group is one ragged
+// element array: the instances' elements are concatenated, their neighbour ids
+// shifted by the instance's offset, and their tiles (the same tiles a single
+// instance would get, so the arithmetic per element is identical) listed one
+// after another, each tile carrying its instance's time step. One launch of the
+// stage kernel per group and stage advances every instance of the group; one
+// CUDA graph holds a whole RK4 step of all groups.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vortex_b200.h"
+#include "vt_common.h"
+#include "vt_launch.h"
+#include "vt_precompute.h"
+
+namespace vt {
+namespace {
+
+std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t bytes) {
+  return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
+// instance AoS (K_i x Np x 4) <-> group SoA rows at an element offset
+__global__ void batch_aos_to_soa(const double2* __restrict__ aos, double2* __restrict__ soa, int K, int Np,
+                                 long long Kpad, long long offset) {
+  const long long l = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (l >= static_cast<long long>(K) * 2 * Np) return;
+  const int e = static_cast<int>(l / (2 * Np)), r = static_cast<int>(l % (2 * Np));
+  soa[r * Kpad + offset + e] = aos[l];
+}
+
+__global__ void batch_soa_to_aos(const double2* __restrict__ soa, double2* __restrict__ aos, int K, int Np,
+                                 long long Kpad, long long offset) {
+  const long long l = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (l >= static_cast<long long>(K) * 2 * Np) return;
+  const int e = static_cast<int>(l / (2 * Np)), r = static_cast<int>(l % (2 * Np));
+  aos[l] = soa[r * Kpad + offset + e];
+}
+
+std::vector<double> fold(int p, int nfq, const vt_mesh_desc& d) {
+  const int Np = np_of(p), NE = p + 1;
+  std::vector<double> ops;
+  for (int dd = 0; dd < 2; ++dd)
+    for (int i = 0; i < Np; ++i)
+      for (int j = 0; j < Np; ++j) {
+        long double s = 0;
+        for (int k = 0; k < Np; ++k)
+          s += static_cast<long double>(d.inv_mass_ref[i * Np + k]) * d.stiffness_ref[(dd * Np + k) * Np + j];
+        ops.push_back(static_cast<double>(s));
+      }
+  for (int sd = 0; sd < 3; ++sd)
+    for (int i = 0; i < Np; ++i)
+      for (int q = 0; q < nfq; ++q) {
+        long double s = 0;
+        for (int j = 0; j < Np; ++j)
+          s += static_cast<long double>(d.inv_mass_ref[i * Np + j]) * d.phi_plus[(sd * Np + j) * nfq + q];
+        ops.push_back(static_cast<double>(s * d.line_quadrature[2 * q + 1]));
+      }
+  for (int sd = 0; sd < 3; ++sd)
+    for (int q = 0; q < nfq; ++q)
+      for (int k = 0; k < NE; ++k) ops.push_back(d.phi_plus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
+  for (int sd = 0; sd < 3; ++sd)
+    for (int q = 0; q < nfq; ++q)
+      for (int k = 0; k < NE; ++k) ops.push_back(d.phi_minus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
+  return ops;
+}
+
+// the reference-space tables that decide which group an instance joins
+std::vector<double> table_key(const vt_mesh_desc& d) {
+  const int Np = np_of(d.p), nfq = d.n_line_points;
+  std::vector<double> k;
+  k.insert(k.end(), d.inv_mass_ref, d.inv_mass_ref + Np * Np);
+  k.insert(k.end(), d.stiffness_ref, d.stiffness_ref + 2 * Np * Np);
+  k.insert(k.end(), d.line_quadrature, d.line_quadrature + 2 * nfq);
+  k.insert(k.end(), d.phi_plus, d.phi_plus + 3 * Np * nfq);
+  k.insert(k.end(), d.phi_minus, d.phi_minus + 3 * Np * nfq);
+  return k;
+}
+
+struct Group {
+  int p = 0, nfq = 0, Np = 0;
+  long long K = 0, Kpad = 0;
+  int ntiles = 0;
+  std::vector<int> members;
+  std::vector<long long> offset;  // element offset of each member
+  std::vector<int> tile_begin;    // first tile of each member
+  std::vector<double> ops;
+  StageKernel kern;
+  int max_blocks = 0;
+  double2 *U = nullptr, *A = nullptr, *Sa = nullptr, *Sb = nullptr, *geo = nullptr;
+  int4 *nbr = nullptr, *tiles = nullptr;
+  int *items = nullptr, *count = nullptr;
+  double* tile_dt = nullptr;
+  unsigned long long* err = nullptr;
+};
+
+}  // namespace
+}  // namespace vt
+
+struct vt_batch {
+  std::mutex mu;
+  int device = 0;
+  int n = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<vt::Group> groups;
+  std::vector<int> group_of, index_in_group, K_of;
+  double2* staging = nullptr;  // largest instance, AoS
+  size_t staging_bytes = 0;
+  cudaGraphExec_t graph = nullptr;
+  int sms = 0, per_sm = 0;
+  std::vector<double> dt;  // per instance
+  int last_instance = -1;
+  vt_error_info last{};
+};
+
+namespace {
+
+using vt::fail;
+
+void release(vt_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto& g : b->groups) {
+    void* bufs[] = {g.U, g.A, g.Sa, g.Sb, g.geo, g.nbr, g.tiles, g.items, g.count, g.tile_dt, g.err};
+    for (void* p : bufs)
+      if (p) cudaFree(p);
+  }
+  if (b->staging) cudaFree(b->staging);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+vt::StageArgs group_args(vt::Group& g, const double2* in, double2* out, int stage, double k_acc, double k_out) {
+  vt::StageArgs a;
+  a.in = in;
+  a.base = g.U;
+  a.acc = g.A;
+  a.out = out;
+  a.geo = g.geo;
+  a.nbr = g.nbr;
+  a.tiles = g.tiles;
+  a.tile_items = g.items;
+  a.tile_count = g.count;
+  a.tile_dt = g.tile_dt;
+  a.err = g.err;
+  a.Kpad = g.Kpad;
+  a.K = static_cast<int>(g.K);
+  a.ntiles = g.ntiles;
+  a.stage = stage;
+  a.c_acc = k_acc;
+  a.c_out = k_out;
+  return a;
+}
+
+// one RK4 step of every group; the coefficients are fractions of each tile's dt
+cudaError_t enqueue_step(vt_batch* b) {
+  cudaError_t e = cudaSuccess;
+  for (int st = 0; st < 4 && !e; ++st)
+    for (auto& g : b->groups) {
+      const double* ops = g.ops.data();
+      switch (st) {
+        case 0: e = g.kern.launch(group_args(g, g.U, g.Sa, 0, 1.0 / 6, 0.5), ops, g.max_blocks, b->stream); break;
+        case 1: e = g.kern.launch(group_args(g, g.Sa, g.Sb, 1, 1.0 / 3, 0.5), ops, g.max_blocks, b->stream); break;
+        case 2: e = g.kern.launch(group_args(g, g.Sb, g.Sa, 2, 1.0 / 3, 1.0), ops, g.max_blocks, b->stream); break;
+        default: e = g.kern.launch(group_args(g, g.Sa, g.U, 3, 0.0, 1.0 / 6), ops, g.max_blocks, b->stream); break;
+      }
+      if (e) break;
+    }
+  return e;
+}
+
+cudaError_t reset_errors(vt_batch* b) {
+  cudaError_t e = cudaSuccess;
+  for (auto& g : b->groups) {
+    if (!e) e = cudaMemsetAsync(g.err, 0xFF, sizeof(unsigned long long), b->stream);
+    if (!e) e = cudaMemsetAsync(g.err + 1, 0, 3 * sizeof(unsigned long long), b->stream);
+  }
+  return e;
+}
+
+int capture(vt_batch* b) {
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  cudaGraph_t gr = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (!e) {
+    const cudaError_t le = enqueue_step(b);
+    e = cudaStreamEndCapture(b->stream, &gr);
+    if (le) e = le;
+  }
+  if (!e) e = cudaGraphInstantiate(&b->graph, gr, 0);
+  if (gr) cudaGraphDestroy(gr);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("batch graph", e)) : VT_OK;
+}
+
+int upload_dt(vt_batch* b) {
+  for (auto& g : b->groups) {
+    std::vector<double> tdt(g.ntiles);
+    for (size_t m = 0; m < g.members.size(); ++m) {
+      const int end = m + 1 < g.members.size() ? g.tile_begin[m + 1] : g.ntiles;
+      for (int t = g.tile_begin[m]; t < end; ++t) tdt[t] = b->dt[g.members[m]];
+    }
+    cudaError_t e =
+        cudaMemcpyAsync(g.tile_dt, tdt.data(), sizeof(double) * g.ntiles, cudaMemcpyHostToDevice, b->stream);
+    if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("batch dt", e));
+    if ((e = cudaStreamSynchronize(b->stream))) return fail(VT_ERR_CUDA, vt::cuda_msg("batch dt", e));
+  }
+  return VT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_batch* vt_batch_create(const vt_mesh_desc* descs, int n, int device, int* status) {
+  auto set = [&](int s) {
+    if (status) *status = s;
+  };
+  if (!descs || n < 1) {
+    set(fail(VT_ERR_INVALID, "vt_batch_create: no instances"));
+    return nullptr;
+  }
+  for (int i = 0; i < n; ++i) {
+    const vt_mesh_desc& d = descs[i];
+    if (!d.element_type || !d.neighbours || !d.det_jacobian || !d.inv_jacobian || !d.normals ||
+        !d.side_lengths || !d.inv_mass_ref || !d.stiffness_ref || !d.line_quadrature || !d.phi_plus ||
+        !d.phi_minus || d.n_elements < 1) {
+      set(fail(VT_ERR_INVALID, "vt_batch_create: incomplete descriptor for instance " + std::to_string(i)));
+      return nullptr;
+    }
+    if (d.p < 0 || d.p > 3 || d.n_line_points < 1 || d.n_line_points > 10) {
+      set(fail(VT_ERR_UNSUPPORTED, "vt_batch_create: p or n_line_points out of range"));
+      return nullptr;
+    }
+    for (int k = 0; k < 3 * d.n_elements; ++k)
+      if (d.neighbours[k] < 0 || d.neighbours[k] >= d.n_elements) {
+        set(fail(VT_ERR_INVALID, "vt_batch_create: neighbour out of range in instance " + std::to_string(i)));
+        return nullptr;
+      }
+  }
+  cudaError_t e = cudaSetDevice(device);
+  if (e) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("cudaSetDevice", e)));
+    return nullptr;
+  }
+  auto* b = new vt_batch();
+  b->device = device;
+  b->n = n;
+  b->group_of.assign(n, -1);
+  b->index_in_group.assign(n, -1);
+  b->K_of.assign(n, 0);
+  b->dt.assign(n, 0.0);
+  // group instances by (p, nfq, reference tables)
+  std::map<std::pair<std::pair<int, int>, std::vector<double>>, int> gid;
+  for (int i = 0; i < n; ++i) {
+    const vt_mesh_desc& d = descs[i];
+    auto key = std::make_pair(std::make_pair(d.p, d.n_line_points), vt::table_key(d));
+    auto it = gid.find(key);
+    int g;
+    if (it == gid.end()) {
+      g = static_cast<int>(b->groups.size());
+      gid.emplace(key, g);
+      b->groups.emplace_back();
+      vt::Group& G = b->groups.back();
+      G.p = d.p;
+      G.nfq = d.n_line_points;
+      G.Np = vt::np_of(d.p);
+      G.ops = vt::fold(d.p, d.n_line_points, d);
+    } else {
+      g = it->second;
+    }
+    vt::Group& G = b->groups[g];
+    b->group_of[i] = g;
+    b->index_in_group[i] = static_cast<int>(G.members.size());
+    b->K_of[i] = d.n_elements;
+    G.members.push_back(i);
+    G.offset.push_back(G.K);
+    G.K += d.n_elements;
+  }
+  if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
+      (e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device))) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_create", e)));
+    release(b);
+    return nullptr;
+  }
+  size_t max_inst_bytes = 0;
+  for (auto& G : b->groups) {
+    G.kern = vt::select_kernel(G.p, G.nfq);
+    int per_sm = 0;
+    if ((e = G.kern.configure(&per_sm))) {
+      set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
+      release(b);
+      return nullptr;
+    }
+    G.max_blocks = b->sms * (per_sm > 0 ? per_sm : 1);
+    G.Kpad = (G.K + 127) / 128 * 128;
+    const long long KP = G.Kpad;
+    // packed geometry, shifted neighbours and per-member tiles
+    std::vector<double2> geo(7 * static_cast<size_t>(KP), make_double2(0.0, 0.0));
+    std::vector<int4> nbr(static_cast<size_t>(KP), make_int4(0, 0, 0, 0));
+    std::vector<int4> tiles;
+    for (size_t m = 0; m < G.members.size(); ++m) {
+      const vt_mesh_desc& d = descs[G.members[m]];
+      const int off = static_cast<int>(G.offset[m]);
+      max_inst_bytes = std::max(max_inst_bytes, sizeof(double) * 4 * static_cast<size_t>(d.n_elements) * G.Np);
+      for (int k = 0; k < d.n_elements; ++k) {
+        const long long n_ = off + k;
+        const double* ji = d.inv_jacobian + 4 * static_cast<size_t>(k);
+        const double* nv = d.normals + 6 * static_cast<size_t>(k);
+        const double* ln = d.side_lengths + 3 * static_cast<size_t>(k);
+        const double det = d.det_jacobian[k];
+        geo[0 * KP + n_] = make_double2(ji[0], ji[1]);
+        geo[1 * KP + n_] = make_double2(ji[2], ji[3]);
+        for (int s = 0; s < 3; ++s) geo[(2 + s) * KP + n_] = make_double2(nv[2 * s], nv[2 * s + 1]);
+        geo[5 * KP + n_] = make_double2(ln[0] / det, ln[1] / det);
+        geo[6 * KP + n_] = make_double2(ln[2] / det, det);
+        const int right = d.neighbours[3 * k] + off, left = d.neighbours[3 * k + 1] + off,
+                  vert = d.neighbours[3 * k + 2] + off;
+        nbr[n_] = d.element_type[k] == 0 ? make_int4(vert, right, left, 0) : make_int4(vert, left, right, 0);
+      }
+      G.tile_begin.push_back(static_cast<int>(tiles.size()));
+      std::vector<int4> runs = vt::structured_tile_runs(d.n_elements, d.element_type, d.neighbours);
+      if (runs.empty())
+        for (int s0 = 0; s0 < d.n_elements; s0 += vt::kTileElems) {
+          const int l0 = std::min(vt::kTileRun, d.n_elements - s0);
+          const int l1 = std::max(0, std::min(vt::kTileRun, d.n_elements - s0 - vt::kTileRun));
+          runs.push_back(make_int4(s0, l0, s0 + vt::kTileRun, l1));
+        }
+      for (const int4& r : runs) tiles.push_back(make_int4(r.x + off, r.y, r.z + off, r.w));
+    }
+    G.ntiles = static_cast<int>(tiles.size());
+    const size_t state_bytes = sizeof(double2) * 2 * G.Np * static_cast<size_t>(KP);
+    if ((e = vt::dalloc(&G.U, state_bytes)) || (e = vt::dalloc(&G.A, state_bytes)) ||
+        (e = vt::dalloc(&G.Sa, state_bytes)) || (e = vt::dalloc(&G.Sb, state_bytes)) ||
+        (e = vt::dalloc(&G.geo, geo.size() * sizeof(double2))) || (e = vt::dalloc(&G.nbr, nbr.size() * sizeof(int4))) ||
+        (e = vt::dalloc(&G.tiles, tiles.size() * sizeof(int4))) ||
+        (e = vt::dalloc(&G.items, sizeof(int) * vt::kMaxItems * tiles.size())) ||
+        (e = vt::dalloc(&G.count, sizeof(int) * tiles.size())) ||
+        (e = vt::dalloc(&G.tile_dt, sizeof(double) * tiles.size())) ||
+        (e = vt::dalloc(&G.err, 4 * sizeof(unsigned long long)))) {
+      set(fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, vt::cuda_msg("vt_batch_create", e)));
+      release(b);
+      return nullptr;
+    }
+    if ((e = cudaMemcpy(G.geo, geo.data(), geo.size() * sizeof(double2), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(G.nbr, nbr.data(), nbr.size() * sizeof(int4), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(G.tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemset(G.U, 0, state_bytes)) || (e = cudaMemset(G.A, 0, state_bytes)) ||
+        (e = cudaMemset(G.Sa, 0, state_bytes)) || (e = cudaMemset(G.Sb, 0, state_bytes)) ||
+        (e = cudaMemset(G.tile_dt, 0, sizeof(double) * tiles.size())) ||
+        (e = vt::launch_build_tile_items(G.tiles, G.nbr, G.items, G.count, G.ntiles, b->stream)) ||
+        (e = cudaStreamSynchronize(b->stream))) {
+      set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_create upload", e)));
+      release(b);
+      return nullptr;
+    }
+  }
+  if ((e = vt::dalloc(&b->staging, max_inst_bytes))) {
+    set(fail(VT_ERR_NO_MEMORY, vt::cuda_msg("vt_batch_create staging", e)));
+    release(b);
+    return nullptr;
+  }
+  b->staging_bytes = max_inst_bytes;
+  set(VT_OK);
+  return b;
+}
+
+void vt_batch_destroy(vt_batch* b) { release(b); }
+
+int vt_batch_size(const vt_batch* b) { return b ? b->n : 0; }
+
+int vt_batch_groups(const vt_batch* b) { return b ? static_cast<int>(b->groups.size()) : 0; }
+
+int vt_batch_upload_state(vt_batch* b, int i, const double* U) {
+  if (!b || !U || i < 0 || i >= b->n) return fail(VT_ERR_INVALID, "vt_batch_upload_state: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  vt::Group& G = b->groups[b->group_of[i]];
+  const int K = b->K_of[i];
+  const size_t bytes = sizeof(double) * 4 * static_cast<size_t>(K) * G.Np;
+  cudaError_t e = cudaMemcpyAsync(b->staging, U, bytes, cudaMemcpyHostToDevice, b->stream);
+  const long long nrow = static_cast<long long>(K) * 2 * G.Np;
+  if (!e) {
+    vt::batch_aos_to_soa<<<static_cast<int>((nrow + 255) / 256), 256, 0, b->stream>>>(
+        b->staging, G.U, K, G.Np, G.Kpad, G.offset[b->index_in_group[i]]);
+    e = cudaGetLastError();
+  }
+  if (!e) e = cudaStreamSynchronize(b->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_upload_state", e)) : VT_OK;
+}
+
+int vt_batch_download_state(vt_batch* b, int i, double* U, double* F) {
+  if (!b || !U || i < 0 || i >= b->n) return fail(VT_ERR_INVALID, "vt_batch_download_state: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  vt::Group& G = b->groups[b->group_of[i]];
+  const int K = b->K_of[i];
+  const size_t bytes = sizeof(double) * 4 * static_cast<size_t>(K) * G.Np;
+  const long long nrow = static_cast<long long>(K) * 2 * G.Np;
+  vt::batch_soa_to_aos<<<static_cast<int>((nrow + 255) / 256), 256, 0, b->stream>>>(
+      G.U, b->staging, K, G.Np, G.Kpad, G.offset[b->index_in_group[i]]);
+  cudaError_t e = cudaGetLastError();
+  if (!e) e = cudaMemcpyAsync(U, b->staging, bytes, cudaMemcpyDeviceToHost, b->stream);
+  if (!e) e = cudaStreamSynchronize(b->stream);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_download_state", e));
+  if (F) vt::flux_from_state(K, G.Np, U, F);
+  return VT_OK;
+}
+
+int vt_batch_set_dt(vt_batch* b, const double* dt) {
+  if (!b || !dt) return fail(VT_ERR_INVALID, "vt_batch_set_dt: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  b->dt.assign(dt, dt + b->n);
+  return upload_dt(b);
+}
+
+int vt_batch_step_rk4(vt_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return fail(VT_ERR_INVALID, "vt_batch_step_rk4: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  cudaError_t e = reset_errors(b);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("batch reset", e));
+  if (!b->graph) {
+    const int st = capture(b);
+    if (st) return st;
+  }
+  for (int s = 0; s < nsteps; ++s)
+    if ((e = cudaGraphLaunch(b->graph, b->stream))) return fail(VT_ERR_CUDA, vt::cuda_msg("batch launch", e));
+  if ((e = cudaStreamSynchronize(b->stream))) return fail(VT_ERR_CUDA, vt::cuda_msg("batch step", e));
+  // first failure over groups: earliest stage, then instance order
+  b->last = vt_error_info{};
+  b->last_instance = -1;
+  unsigned long long best_epoch = ~0ull;
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    vt::Group& G = b->groups[gi];
+    unsigned long long w[4];
+    if ((e = cudaMemcpy(w, G.err, sizeof(w), cudaMemcpyDeviceToHost))) return fail(VT_ERR_CUDA, "batch errors");
+    if (w[3] & 2ull) return fail(VT_ERR_CUDA, "stage kernel: a bulk-copy wait gave up (the state is not valid)");
+    if (w[0] == ~0ull) continue;
+    const unsigned long long epoch = w[0] >> 40;
+    unsigned long long local = w[0] & ((1ull << 40) - 1);
+    vt_error_info info{};
+    info.code = static_cast<int>(local & 3ull);
+    local >>= 2;
+    info.side = static_cast<int>(local % 3ull);
+    local /= 3ull;
+    info.point = static_cast<int>(local % static_cast<unsigned long long>(G.nfq));
+    const long long ge = static_cast<long long>(local / static_cast<unsigned long long>(G.nfq));
+    const size_t m = std::upper_bound(G.offset.begin(), G.offset.end(), ge) - G.offset.begin() - 1;
+    info.element = static_cast<int>(ge - G.offset[m]);
+    info.step = static_cast<int64_t>(epoch / 4);
+    info.stage = static_cast<int>(epoch % 4);
+    const int inst = G.members[m];
+    if (epoch < best_epoch || (epoch == best_epoch && inst < b->last_instance)) {
+      best_epoch = epoch;
+      b->last = info;
+      b->last_instance = inst;
+    }
+  }
+  if (b->last_instance < 0) return VT_OK;
+  return fail(b->last.code, "Non-physical state (code " + std::to_string(b->last.code) + ") in instance " +
+                                std::to_string(b->last_instance) + " at element " + std::to_string(b->last.element));
+}
+
+int vt_batch_last_error(const vt_batch* b, int* instance, vt_error_info* out) {
+  if (!b || !out) return fail(VT_ERR_INVALID, "bad argument");
+  *out = b->last;
+  if (instance) *instance = b->last_instance;
+  return VT_OK;
+}
+
+int vt_batch_autotune(vt_batch* b, int trials, int* blocks_per_sm_out) {
+  if (!b || trials < 1) return fail(VT_ERR_INVALID, "vt_batch_autotune: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  // candidate persistent grids per group: SMs x {1, 2, 3} blocks; the state is
+  // restored afterwards so tuning does not advance the solution
+  std::vector<std::vector<double2>> saved;
+  for (auto& G : b->groups) {
+    const size_t state = 2 * G.Np * static_cast<size_t>(G.Kpad);
+    saved.emplace_back(state);
+    if (cudaMemcpy(saved.back().data(), G.U, state * sizeof(double2), cudaMemcpyDeviceToHost))
+      return fail(VT_ERR_CUDA, "autotune save");
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    vt::Group& G = b->groups[gi];
+    int best_b = 1;
+    float best_ms = 1e30f;
+    int limit = 0;
+    G.kern.configure(&limit);
+    for (int bps = 1; bps <= std::max(1, limit); ++bps) {
+      G.max_blocks = b->sms * bps;
+      float tot = 0;
+      for (int r = 0; r < trials + 1; ++r) {
+        cudaEventRecord(e0, b->stream);
+        for (int st = 0; st < 4; ++st) {
+          const vt::StageArgs a = group_args(G, st == 0 ? G.U : (st == 2 ? G.Sb : G.Sa),
+                                             st == 0 ? G.Sa : (st == 1 ? G.Sb : (st == 2 ? G.Sa : G.U)), st,
+                                             st == 0 ? 1.0 / 6 : (st == 3 ? 0.0 : 1.0 / 3),
+                                             st == 0 ? 0.5 : (st == 1 ? 0.5 : (st == 2 ? 1.0 : 1.0 / 6)));
+          G.kern.launch(a, G.ops.data(), G.max_blocks, b->stream);
+        }
+        cudaEventRecord(e1, b->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r) tot += ms;  // first repetition warms up
+      }
+      if (tot < best_ms) {
+        best_ms = tot;
+        best_b = bps;
+      }
+    }
+    G.max_blocks = b->sms * best_b;
+    if (blocks_per_sm_out) blocks_per_sm_out[gi] = best_b;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    vt::Group& G = b->groups[gi];
+    if (cudaMemcpy(G.U, saved[gi].data(), saved[gi].size() * sizeof(double2), cudaMemcpyHostToDevice))
+      return fail(VT_ERR_CUDA, "autotune restore");
+  }
+  return capture(b);
+}
+
+int vt_batch_set_blocks_per_sm(vt_batch* b, const int* blocks_per_sm) {
+  if (!b || !blocks_per_sm) return fail(VT_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    int limit = 0;
+    b->groups[gi].kern.configure(&limit);
+    const int bps = std::max(1, std::min(blocks_per_sm[gi], std::max(1, limit)));
+    b->groups[gi].max_blocks = b->sms * bps;
+  }
+  return capture(b);
+}
+
+int vt_batch_group_info(const vt_batch* b, int g, int* p, int* n_instances, int64_t* n_elements) {
+  if (!b || g < 0 || g >= static_cast<int>(b->groups.size())) return fail(VT_ERR_INVALID, "bad group");
+  if (p) *p = b->groups[g].p;
+  if (n_instances) *n_instances = static_cast<int>(b->groups[g].members.size());
+  if (n_elements) *n_elements = b->groups[g].K;
+  return VT_OK;
+}
+
+}  // extern "C"

@@ -66,6 +66,7 @@ struct StageArgs {
   const int4* tiles;
   const int* tile_items;
   const int* tile_count;
+  const double* tile_dt;  // per-tile time step (batched problems), or null: c_* hold dt
   unsigned long long* err;  // [0] first-error key, [1] steps done, [2] blocks done
   long long Kpad;
   int K;

@@ -234,6 +234,7 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     a.nbr = nbr;
     a.tiles = tiles;
     a.tile_items = items;
+    a.tile_dt = nullptr;
     a.tile_count = count;
     a.ntiles = cv.ntiles;
     a.err = errw;
@@ -245,10 +246,10 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     return a;
   };
   for (int s = 0; s < nsteps && !e; ++s) {
-    if (!e) e = pk.launch(args(U, Sa, 0, dt / 6, dt / 2), ops, max_blocks, st);
-    if (!e) e = pk.launch(args(Sa, Sb, 1, dt / 3, dt / 2), ops, max_blocks, st);
-    if (!e) e = pk.launch(args(Sb, Sa, 2, dt / 3, dt), ops, max_blocks, st);
-    if (!e) e = pk.launch(args(Sa, U, 3, 0.0, dt / 6), ops, max_blocks, st);
+    if (!e) e = pk.launch(args(U, Sa, 0, (1.0 / 6) * dt, 0.5 * dt), ops, max_blocks, st);
+    if (!e) e = pk.launch(args(Sa, Sb, 1, (1.0 / 3) * dt, 0.5 * dt), ops, max_blocks, st);
+    if (!e) e = pk.launch(args(Sb, Sa, 2, (1.0 / 3) * dt, dt), ops, max_blocks, st);
+    if (!e) e = pk.launch(args(Sa, U, 3, 0.0, (1.0 / 6) * dt), ops, max_blocks, st);
   }
   if (!e) {
     vt::scatter_aos_kernel<<<tb, 256, 0, st>>>(U, reinterpret_cast<double2*>(dU_out), K, Np, cv.Kpad);

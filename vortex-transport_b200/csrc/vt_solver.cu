@@ -195,6 +195,7 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
   a.nbr = c->nbr;
   a.tiles = c->tiles;
   a.tile_items = c->tile_items;
+  a.tile_dt = nullptr;
   a.tile_count = c->tile_count;
   a.ntiles = c->ntiles;
   a.err = c->err;
@@ -209,10 +210,10 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
 cudaError_t enqueue_rk4_step(vt_ctx* c, double dt) {
   cudaError_t e;
   const double* ops = c->ops.data();
-  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2), ops, c->max_blocks, c->stream))) return e;
-  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2), ops, c->max_blocks, c->stream))) return e;
-  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt), ops, c->max_blocks, c->stream))) return e;
-  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6), ops, c->max_blocks, c->stream);
+  if ((e = c->launch(stage_args(c, c->U, c->U, c->A, c->Sa, 0, (1.0 / 6) * dt, 0.5 * dt), ops, c->max_blocks, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, (1.0 / 3) * dt, 0.5 * dt), ops, c->max_blocks, c->stream))) return e;
+  if ((e = c->launch(stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, (1.0 / 3) * dt, dt), ops, c->max_blocks, c->stream))) return e;
+  return c->launch(stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, (1.0 / 6) * dt), ops, c->max_blocks, c->stream);
 }
 
 cudaError_t reset_error_words(vt_ctx* c) {
@@ -582,10 +583,10 @@ int vt_profile_rk4_stages(vt_ctx* c, double dt, int reps, float* ms) {
   cudaError_t e = reset_error_words(c);
   const double* ops = c->ops.data();
   for (int r = 0; r < reps && !e; ++r) {
-    const vt::StageArgs args[4] = {stage_args(c, c->U, c->U, c->A, c->Sa, 0, dt / 6, dt / 2),
-                                   stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, dt / 3, dt / 2),
-                                   stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, dt / 3, dt),
-                                   stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, dt / 6)};
+    const vt::StageArgs args[4] = {stage_args(c, c->U, c->U, c->A, c->Sa, 0, (1.0 / 6) * dt, 0.5 * dt),
+                                   stage_args(c, c->Sa, c->U, c->A, c->Sb, 1, (1.0 / 3) * dt, 0.5 * dt),
+                                   stage_args(c, c->Sb, c->U, c->A, c->Sa, 2, (1.0 / 3) * dt, dt),
+                                   stage_args(c, c->Sa, c->U, c->A, c->U, 3, 0.0, (1.0 / 6) * dt)};
     cudaEventRecord(ev[0], c->stream);
     for (int s = 0; s < 4 && !e; ++s) {
       e = c->launch(args[s], ops, c->max_blocks, c->stream);

@@ -410,6 +410,8 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
 
     // ---- 6b. stage update: component c of every node ----------------------------------
     if (valid) {
+      const double dtt = a.tile_dt ? __ldg(a.tile_dt + tile) : 1.0;
+      const double c_acc = a.c_acc * dtt, c_out = a.c_out * dtt;
       const int h = c >> 1, part = c & 1;
       const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
       const double* in = reinterpret_cast<const double*>(a.in) + off0;
@@ -422,25 +424,25 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
             const double u = __ldg(in + i * step);
-            acc[i * step] = fma(a.c_acc, r[i], u);
-            out[i * step] = fma(a.c_out, r[i], u);
+            acc[i * step] = fma(c_acc, r[i], u);
+            out[i * step] = fma(c_out, r[i], u);
           }
           break;
         case 1:
         case 2:
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
-            acc[i * step] = fma(a.c_acc, r[i], acc[i * step]);
-            out[i * step] = fma(a.c_out, r[i], __ldg(base + i * step));
+            acc[i * step] = fma(c_acc, r[i], acc[i * step]);
+            out[i * step] = fma(c_out, r[i], __ldg(base + i * step));
           }
           break;
         case 3:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = fma(a.c_out, r[i], acc[i * step]);
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], acc[i * step]);
           break;
         case kStageEuler:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = fma(a.c_out, r[i], __ldg(in + i * step));
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], __ldg(in + i * step));
           break;
         default:
 #pragma unroll
