@@ -74,7 +74,7 @@ def test_batch_autotune_keeps_state_and_caches(vt, tmp_path):
 
 
 def test_ensemble_dt_factor_is_stable(vt):
-    """A slice of the seeded ensemble runs its 500 steps at dt = 0.02 h/(2p+1)."""
+    """A slice of the seeded ensemble runs its 500 steps at the stable time step."""
     from vortex_transport_b200 import workloads
     inst = workloads.ensemble_instances(n=12, seed=1)
     pbs = workloads.build_problems(inst)

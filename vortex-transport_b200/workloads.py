@@ -14,10 +14,18 @@ import numpy as np
 
 from . import Problem, make_params, vortex
 
-# RK4 with the reference's Roe flux (whose dissipation speed is c^4, not c)
-# blows up at dt = 0.1 h / (2p + 1) and 0.05 h / (2p + 1) in the reference
-# itself; 0.02 h / (2p + 1) is stable for every mesh and order of the ensemble.
-ENSEMBLE_DT_FACTOR = 0.02
+# The reference's Roe flux dissipates with speed ci = c2^2 (Numericalflux.cpp:117)
+# instead of c, and the free-stream c^2 = gamma p/rho = 1/M^2 for this vortex,
+# so the fastest wave is about |u| + M^-4 (17 at M = 0.5, 124 at M = 0.3). RK4 at
+# the configuration's dt = 0.1 h/(2p+1) blows up in the reference itself; here
+# dt = C h / ((2p+1) (1 + M^-4)) with C = 0.3, which is 0.018 h/(2p+1) at
+# M = 0.5 (the reference is stable up to ~0.03 there) and scales with M^4.
+ENSEMBLE_CFL = 0.3
+
+
+def stable_dt(side: int, p: int, M_infty: float, cfl: float = ENSEMBLE_CFL, domain: float = 10.0) -> float:
+    h = domain / side
+    return cfl * h / ((2 * p + 1) * (1.0 + M_infty ** -4))
 
 
 @dataclass
@@ -32,21 +40,23 @@ class Instance:
     dt: float
 
 
-def ensemble_instances(n: int = 512, seed: int = 1, dt_factor: float = ENSEMBLE_DT_FACTOR,
+def ensemble_instances(n: int = 512, seed: int = 1, cfl: float = ENSEMBLE_CFL,
                        sides=(16, 32, 48, 64, 96, 128), orders=(1, 2, 3)) -> list[Instance]:
     """The batched-ensemble configuration: eps ~ U[0.1, 0.5], M ~ U[0.3, 0.7],
     centre ~ U[-2, 2]^2 on the 10x10 periodic domain, mesh side drawn from
-    `sides`, p from `orders`, perturb_grid ~ U[0, 0.2], all from `seed`;
-    dt = dt_factor * h / (2p + 1) with h = 10 / side."""
+    `sides`, p from `orders`, perturb_grid ~ U[0, 0.2], all from `seed`; the
+    time step is stable_dt (see ENSEMBLE_CFL)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
         side = int(rng.choice(sides))
         p = int(rng.choice(orders))
-        out.append(Instance(side=side, p=p, perturb=float(rng.uniform(0.0, 0.2)),
-                            epsilon=float(rng.uniform(0.1, 0.5)), M_infty=float(rng.uniform(0.3, 0.7)),
-                            x0=float(rng.uniform(-2, 2)), y0=float(rng.uniform(-2, 2)),
-                            dt=dt_factor * (10.0 / side) / (2 * p + 1)))
+        perturb = float(rng.uniform(0.0, 0.2))
+        eps = float(rng.uniform(0.1, 0.5))
+        mach = float(rng.uniform(0.3, 0.7))
+        x0, y0 = float(rng.uniform(-2, 2)), float(rng.uniform(-2, 2))
+        out.append(Instance(side=side, p=p, perturb=perturb, epsilon=eps, M_infty=mach, x0=x0, y0=y0,
+                            dt=stable_dt(side, p, mach, cfl)))
     return out
 
 
