@@ -220,6 +220,63 @@ int vt_batch_autotune(vt_batch* batch, int trials, int* blocks_per_sm);
 /* Applies a stored tuning (as reported by vt_batch_autotune). */
 int vt_batch_set_blocks_per_sm(vt_batch* batch, const int* blocks_per_sm);
 
+/* ---- discrete adjoint ---------------------------------------------------- */
+/* No counterpart in the reference (which has no derivatives). The exact
+ * transpose of the linearised RK4 step of vt_step_rk4: per stage the
+ * transposed volume operator and nodal-flux Jacobian, the transposed Roe-flux
+ * Jacobian at every face point (Roe averages, the c2^2 speed and the entropy
+ * fix differentiated, Numericalflux.cpp:99-156), the transposed lift and mass
+ * inverse, and the reversed RK4 combine. States are (K x Np x 4) arrays in the
+ * reference layout, host memory unless `device_pointers` is non-zero (then
+ * device memory on the context's device). Needs a mesh whose side s faces its
+ * neighbour's side s (the reference mesh does); VT_ERR_UNSUPPORTED otherwise. */
+
+/* Schedule of the binomial checkpointing of an nsteps-step run with
+ * `nsnapshots` stored states (U_0 included). */
+typedef struct vt_checkpoint_info {
+  int64_t advance_steps;         /* plain RK4 steps, forward sweep included */
+  int64_t forward_sweep_steps;   /* of which in the forward sweep (nsteps - 1) */
+  int64_t stage_steps;           /* steps rerun keeping stage states (= nsteps) */
+  int64_t adjoint_steps;         /* = nsteps */
+  int64_t optimal_advance_steps; /* Griewank's bound r n - C(S + r, S + 1) */
+  int32_t slots_used;            /* snapshot buffers actually used */
+} vt_checkpoint_info;
+
+/* Plans the reversal on the host only (no device needed). */
+int vt_checkpoint_plan(int nsteps, int nsnapshots, vt_checkpoint_info* out);
+
+/* Forward sweep: nsteps RK4 steps of size dt from the current state, keeping
+ * at most `nsnapshots` states in device memory (nsnapshots >= nsteps keeps
+ * every step's start). On return the context holds U(T) exactly as
+ * vt_step_rk4 would leave it and the time has advanced; a non-physical state
+ * returns its code. */
+int vt_adjoint_forward(vt_ctx* ctx, double dt, int nsteps, int nsnapshots);
+/* Reverse sweep of the last vt_adjoint_forward: given dJ/dU(T) returns
+ * dJ/dU(0), recomputing the steps between checkpoints. Leaves the state and
+ * the time alone, and may be called again with another dJ/dU(T). */
+int vt_adjoint_backward(vt_ctx* ctx, const double* dJdU_T, double* dJdU_0, int device_pointers);
+/* Schedule of the last vt_adjoint_forward. */
+int vt_adjoint_info(const vt_ctx* ctx, vt_checkpoint_info* out);
+
+/* Directional derivative of the right-hand side at U along V, dR = R'(U) V
+ * (forward mode on dual numbers), and the transpose product G = R'(U)^T W
+ * through the adjoint kernels. The context's state is not touched. */
+int vt_rhs_jvp(vt_ctx* ctx, const double* U, const double* V, double* dR, int device_pointers);
+int vt_rhs_vjp(vt_ctx* ctx, const double* U, const double* W, double* G, int device_pointers);
+/* Tangent-linear model: advances the state nsteps RK4 steps as vt_step_rk4
+ * does and carries a perturbation along: dU_T = (dU(T)/dU(0)) dU_0. */
+int vt_tangent_rk4(vt_ctx* ctx, double dt, int nsteps, const double* dU_0, double* dU_T, int device_pointers);
+
+/* Host-side pointwise pieces, for checks: the Roe flux in the algebra of the
+ * stage kernels (Numericalflux.cpp:13-157; returns 0 or the non-physical code
+ * 1/2/3), its Jacobian-vector product, and its transpose product (which adds
+ * to buL and buR). */
+int vt_roe_flux(const double* uL, const double* uR, double nx, double ny, double* flux);
+int vt_roe_flux_jvp(const double* uL, const double* uR, double nx, double ny, const double* duL,
+                    const double* duR, double* dflux);
+void vt_roe_flux_vjp(const double* uL, const double* uR, double nx, double ny, const double* bflux, double* buL,
+                     double* buR);
+
 /* ---- stepping without device allocation --------------------------------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc:
  * code running while a host framework's pool or arena owns all device memory,

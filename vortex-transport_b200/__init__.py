@@ -86,6 +86,15 @@ class vt_device_mesh(ctypes.Structure):
                 ("line_quadrature", _dp), ("phi_plus", _dp), ("phi_minus", _dp)]
 
 
+class vt_checkpoint_info(ctypes.Structure):
+    _fields_ = [("advance_steps", ctypes.c_int64), ("forward_sweep_steps", ctypes.c_int64),
+                ("stage_steps", ctypes.c_int64), ("adjoint_steps", ctypes.c_int64),
+                ("optimal_advance_steps", ctypes.c_int64), ("slots_used", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 class VortexError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"[{status}] {message}")
@@ -156,6 +165,19 @@ _SIGNATURES = {
                                            ctypes.POINTER(vt_error_info)]),
     "vt_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "vt_batch_set_blocks_per_sm": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "vt_checkpoint_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "vt_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "vt_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "vt_adjoint_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "vt_rhs_jvp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_int]),
+    "vt_rhs_vjp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_int]),
+    "vt_tangent_rk4": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_int]),
+    "vt_roe_flux": (ctypes.c_int, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp]),
+    "vt_roe_flux_jvp": (ctypes.c_int, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]),
+    "vt_roe_flux_vjp": (None, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]),
     "vt_noalloc_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     "vt_step_rk4_noalloc": (ctypes.c_int, [ctypes.POINTER(vt_device_mesh), ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
@@ -266,6 +288,46 @@ def flux_from_state(U: np.ndarray) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # host precompute
 # ---------------------------------------------------------------------------
+def _is_cuda_tensor(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+def checkpoint_plan(nsteps: int, nsnapshots: int) -> dict:
+    """Schedule of the binomial checkpointing of an nsteps-step adjoint run
+    with nsnapshots stored states (host only)."""
+    info = vt_checkpoint_info()
+    _check(lib().vt_checkpoint_plan(int(nsteps), int(nsnapshots), ctypes.byref(info)))
+    return info.as_dict()
+
+
+def _vec4(x) -> np.ndarray:
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+    assert x.shape == (4,), x.shape
+    return x
+
+
+def roe_flux(uL, uR, n):
+    """(flux, code): the Roe flux in the stage kernels' algebra, on the host."""
+    f = np.empty(4)
+    code = lib().vt_roe_flux(_ptr(_vec4(uL)), _ptr(_vec4(uR)), float(n[0]), float(n[1]), _ptr(f))
+    return f, code
+
+
+def roe_flux_jvp(uL, uR, n, duL, duR) -> np.ndarray:
+    df = np.empty(4)
+    lib().vt_roe_flux_jvp(_ptr(_vec4(uL)), _ptr(_vec4(uR)), float(n[0]), float(n[1]), _ptr(_vec4(duL)),
+                          _ptr(_vec4(duR)), _ptr(df))
+    return df
+
+
+def roe_flux_vjp(uL, uR, n, bflux):
+    """(buL, buR) = transposed Roe Jacobian applied to bflux."""
+    buL, buR = np.zeros(4), np.zeros(4)
+    lib().vt_roe_flux_vjp(_ptr(_vec4(uL)), _ptr(_vec4(uR)), float(n[0]), float(n[1]), _ptr(_vec4(bflux)),
+                          _ptr(buL), _ptr(buR))
+    return buL, buR
+
+
 _ARRAY_SHAPES = {
     "vertices": lambda i: (i.K, 3, 2), "conn": lambda i: (i.K, 3), "type": lambda i: (i.K,),
     "nodes_ref": lambda i: (i.Np, 2), "nodes_phys": lambda i: (i.K, i.Np, 2),
@@ -428,6 +490,60 @@ class Solver:
     def totals(self) -> np.ndarray:
         out = np.empty(4)
         _check(lib().vt_totals(self._h, _ptr(out)))
+        return out
+
+    # derivatives ------------------------------------------------------------
+    # Arrays are (K, Np, 4) float64: numpy arrays (host) or CUDA torch tensors
+    # on this solver's device (passed as device pointers); results come back in
+    # the same kind as the first array argument.
+    def _state_args(self, *arrays):
+        dev = _is_cuda_tensor(arrays[0])
+        if dev:
+            import torch
+            torch.cuda.current_stream(arrays[0].device).synchronize()
+            keep = [a.detach().to(torch.float64).contiguous() for a in arrays]
+            for a in keep:
+                assert tuple(a.shape) == (self.K, self.Np, 4), a.shape
+            out = torch.empty_like(keep[0])
+            return [ctypes.c_void_p(a.data_ptr()) for a in keep], ctypes.c_void_p(out.data_ptr()), out, 1, keep
+        keep = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in arrays]
+        for a in keep:
+            assert a.shape == (self.K, self.Np, 4), a.shape
+        out = np.empty((self.K, self.Np, 4))
+        return ([a.ctypes.data_as(ctypes.c_void_p) for a in keep], out.ctypes.data_as(ctypes.c_void_p), out, 0,
+                keep)
+
+    def adjoint_forward(self, dt: float, nsteps: int, nsnapshots: int) -> None:
+        """nsteps RK4 steps keeping checkpoints for adjoint_backward."""
+        self._step_status(lib().vt_adjoint_forward(self._h, float(dt), int(nsteps), int(nsnapshots)))
+
+    def adjoint_backward(self, dJdU_T):
+        """dJ/dU(0) from dJ/dU(T), for the last adjoint_forward."""
+        ins, outp, out, dev, _keep = self._state_args(dJdU_T)
+        self._step_status(lib().vt_adjoint_backward(self._h, ins[0], outp, dev))
+        return out
+
+    def adjoint_info(self) -> dict:
+        info = vt_checkpoint_info()
+        _check(lib().vt_adjoint_info(self._h, ctypes.byref(info)))
+        return info.as_dict()
+
+    def rhs_jvp(self, U, V):
+        """R'(U) V."""
+        ins, outp, out, dev, _keep = self._state_args(U, V)
+        _check(lib().vt_rhs_jvp(self._h, ins[0], ins[1], outp, dev))
+        return out
+
+    def rhs_vjp(self, U, W):
+        """R'(U)^T W."""
+        ins, outp, out, dev, _keep = self._state_args(U, W)
+        _check(lib().vt_rhs_vjp(self._h, ins[0], ins[1], outp, dev))
+        return out
+
+    def tangent_rk4(self, dt: float, nsteps: int, dU0):
+        """Advances the state nsteps RK4 steps and returns the propagated dU0."""
+        ins, outp, out, dev, _keep = self._state_args(dU0)
+        self._step_status(lib().vt_tangent_rk4(self._h, float(dt), int(nsteps), ins[0], outp, dev))
         return out
 
     def profile_stages(self, dt: float, reps: int) -> np.ndarray:

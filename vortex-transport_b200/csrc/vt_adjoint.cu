@@ -1,0 +1,453 @@
+// Discrete adjoint of the RK4 stepper, its tangent-linear model and the
+// checkpointed reverse sweep (C ABI in include/vortex_b200.h, "discrete adjoint").
+//
+// Forward sweep: the plain RK4 step (the stage kernel of vt_step_rk4, launched
+// on explicit buffers) advances between checkpoint slots as the binomial plan
+// of vt_checkpoint.h says. Reverse sweep, per step i = n-1 .. 0: rerun step i
+// from its checkpoint keeping the stage states U1, U2, U3, then four reverse
+// stages (adjoint_face_kernel + adjoint_element_kernel each) turn the adjoint
+// of U_{i+1} into the adjoint of U_i:
+//   a4 = dt/6 lam                 g4 = R'(U3)^T a4
+//   a3 = dt/3 lam + dt   g4       g3 = R'(U2)^T a3
+//   a2 = dt/3 lam + dt/2 g3       g2 = R'(U1)^T a2
+//   a1 = dt/6 lam + dt/2 g2       g1 = R'(U_i)^T a1
+//   lam <- lam + g4 + g3 + g2 + g1
+// with the coefficients the forward stages use (Timestepping.cpp:128-305).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vortex_b200.h"
+#include "vt_adjoint_kernels.cuh"
+#include "vt_checkpoint.h"
+#include "vt_common.h"
+#include "vt_ctx.h"
+
+namespace vt {
+namespace {
+
+using FaceFn = cudaError_t (*)(const AdjArgs&, const double*, cudaStream_t);
+using JvpFn = cudaError_t (*)(const double2*, const double2*, double2*, const double2*, const int4*, long long,
+                              int, const double*, cudaStream_t);
+
+struct AdjKernels {
+  FaceFn face = nullptr;
+  FaceFn element = nullptr;
+  JvpFn jvp = nullptr;
+};
+
+template <int P, int NFQ>
+cudaError_t launch_face(const AdjArgs& a, const double* ops, cudaStream_t st) {
+  StageOps<P, NFQ> o;
+  std::memcpy(&o, ops, sizeof(o));
+  const dim3 grid((a.K + kAdjRun - 1) / kAdjRun, 3), block(kAdjRun, NFQ);
+  adjoint_face_kernel<P, NFQ><<<grid, block, 0, st>>>(a, o);
+  return cudaGetLastError();
+}
+
+template <int P, int NFQ>
+cudaError_t launch_element(const AdjArgs& a, const double* ops, cudaStream_t st) {
+  StageOps<P, NFQ> o;
+  std::memcpy(&o, ops, sizeof(o));
+  const dim3 grid((a.K + kAdjRun - 1) / kAdjRun), block(kAdjRun, np_of_p(P));
+  adjoint_element_kernel<P, NFQ><<<grid, block, 0, st>>>(a, o);
+  return cudaGetLastError();
+}
+
+template <int P, int NFQ>
+cudaError_t launch_jvp(const double2* U, const double2* V, double2* dR, const double2* geo, const int4* nbr,
+                       long long KP, int K, const double* ops, cudaStream_t st) {
+  StageOps<P, NFQ> o;
+  std::memcpy(&o, ops, sizeof(o));
+  rhs_jvp_kernel<P, NFQ><<<(K + 127) / 128, 128, 0, st>>>(U, V, dR, geo, nbr, KP, K, o);
+  return cudaGetLastError();
+}
+
+template <int P, int NFQ>
+AdjKernels kernels_of() {
+  return AdjKernels{launch_face<P, NFQ>, launch_element<P, NFQ>, launch_jvp<P, NFQ>};
+}
+
+template <int P>
+AdjKernels kernels_for_nfq(int nfq) {
+  switch (nfq) {
+    case 1: return kernels_of<P, 1>();
+    case 2: return kernels_of<P, 2>();
+    case 3: return kernels_of<P, 3>();
+    case 4: return kernels_of<P, 4>();
+    case 5: return kernels_of<P, 5>();
+    case 6: return kernels_of<P, 6>();
+    case 7: return kernels_of<P, 7>();
+    case 8: return kernels_of<P, 8>();
+    case 9: return kernels_of<P, 9>();
+    case 10: return kernels_of<P, 10>();
+    default: return AdjKernels{};
+  }
+}
+
+AdjKernels select_adjoint(int p, int nfq) {
+  switch (p) {
+    case 0: return kernels_for_nfq<0>(nfq);
+    case 1: return kernels_for_nfq<1>(nfq);
+    case 2: return kernels_for_nfq<2>(nfq);
+    case 3: return kernels_for_nfq<3>(nfq);
+    default: return AdjKernels{};
+  }
+}
+
+}  // namespace
+
+struct AdjointState {
+  AdjKernels k;
+  size_t state_elems = 0;  // double2 entries of one state vector
+  // work, stage states, adjoint, accumulator, two stage adjoints (contiguous)
+  double2* bufs = nullptr;
+  double2 *work = nullptr, *s1 = nullptr, *s2 = nullptr, *s3 = nullptr;
+  double2 *lam = nullptr, *acc = nullptr, *a0 = nullptr, *a1 = nullptr;
+  double2 *bp = nullptr, *bm = nullptr;  // face adjoints
+  double2* slots = nullptr;
+  int nslots = 0;
+  // last forward sweep
+  std::vector<CkptAction> plan;
+  size_t first_adjoint = 0;
+  double dt = 0.0;
+  int nsteps = 0;
+  bool have_forward = false;
+  bool fresh = false;  // the forward sweep's checkpoints and stage states are intact
+  vt_checkpoint_info info{};
+};
+
+namespace {
+
+int setup(vt_ctx* c) {
+  if (c->adj) return VT_OK;
+  if (!c->side_pairing)
+    return fail(VT_ERR_UNSUPPORTED, "adjoint: side s of some element does not face side s of its neighbour");
+  auto* s = new AdjointState();
+  s->k = select_adjoint(c->p, c->nfq);
+  if (!s->k.face) {
+    delete s;
+    return fail(VT_ERR_UNSUPPORTED, "adjoint: unsupported (p, nfq)");
+  }
+  s->state_elems = static_cast<size_t>(2 * c->Np) * static_cast<size_t>(c->Kpad);
+  const size_t face_elems = static_cast<size_t>(6 * c->nfq) * static_cast<size_t>(c->Kpad);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s->bufs), sizeof(double2) * (8 * s->state_elems + 2 * face_elems));
+  if (!e) e = cudaMemsetAsync(s->bufs, 0, sizeof(double2) * (8 * s->state_elems + 2 * face_elems), c->stream);
+  if (e) {
+    delete s;
+    return fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, cuda_msg("adjoint buffers", e));
+  }
+  double2** named[8] = {&s->work, &s->s1, &s->s2, &s->s3, &s->lam, &s->acc, &s->a0, &s->a1};
+  for (int i = 0; i < 8; ++i) *named[i] = s->bufs + i * s->state_elems;
+  s->bp = s->bufs + 8 * s->state_elems;
+  s->bm = s->bp + face_elems;
+  c->adj = s;
+  return VT_OK;
+}
+
+int ensure_slots(vt_ctx* c, int n) {
+  AdjointState* s = c->adj;
+  if (s->nslots >= n) return VT_OK;
+  if (s->slots) cudaFree(s->slots);
+  s->slots = nullptr;
+  s->nslots = 0;
+  const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s->slots), sizeof(double2) * s->state_elems * n);
+  if (e) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA,
+                cuda_msg(("adjoint: " + std::to_string(n) + " checkpoint states").c_str(), e));
+  }
+  s->nslots = n;
+  return VT_OK;
+}
+
+double2* slot(vt_ctx* c, int i) {
+  return i == kWorkSlot ? c->adj->work : c->adj->slots + static_cast<size_t>(i) * c->adj->state_elems;
+}
+
+cudaError_t stage(vt_ctx* c, const double2* in, const double2* base, double2* out, int st, double ca, double co) {
+  return c->launch(stage_args(c, in, base, c->A, out, st, ca, co), c->ops.data(), c->max_blocks, c->stream);
+}
+
+// One plain RK4 step from X into Y (Y may be X), stages through Sa, Sb.
+cudaError_t plain_step(vt_ctx* c, const double2* X, double2* Y, double dt) {
+  cudaError_t e;
+  if ((e = stage(c, X, X, c->Sa, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
+  if ((e = stage(c, c->Sa, X, c->Sb, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
+  if ((e = stage(c, c->Sb, X, c->Sa, 2, (1.0 / 3) * dt, dt))) return e;
+  return stage(c, c->Sa, X, Y, 3, 0.0, (1.0 / 6) * dt);
+}
+
+cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt) {
+  cudaError_t e = plain_step(c, X, Y, dt);
+  for (int i = 1; i < k && !e; ++i) e = plain_step(c, Y, Y, dt);
+  return e;
+}
+
+// Step from X keeping the stage states in s1, s2, s3; the new state goes to
+// `out` when given (else the last stage is not run).
+cudaError_t stage_step(vt_ctx* c, const double2* X, double dt, double2* out) {
+  AdjointState* s = c->adj;
+  cudaError_t e;
+  if ((e = stage(c, X, X, s->s1, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
+  if ((e = stage(c, s->s1, X, s->s2, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
+  if ((e = stage(c, s->s2, X, s->s3, 2, (1.0 / 3) * dt, dt))) return e;
+  return out ? stage(c, s->s3, X, out, 3, 0.0, (1.0 / 6) * dt) : cudaSuccess;
+}
+
+AdjArgs adj_args(vt_ctx* c) {
+  AdjArgs a{};
+  a.bp = c->adj->bp;
+  a.bm = c->adj->bm;
+  a.geo = c->geo;
+  a.nbr = c->nbr;
+  a.Kpad = c->Kpad;
+  a.K = c->K;
+  a.sa = 1.0;
+  return a;
+}
+
+cudaError_t reverse_stage(vt_ctx* c, const AdjArgs& a) {
+  cudaError_t e = c->adj->k.face(a, c->ops.data(), c->stream);
+  return e ? e : c->adj->k.element(a, c->ops.data(), c->stream);
+}
+
+// lam <- adjoint of U_i given lam = adjoint of U_{i+1}; X = U_i, stage states in s1..s3.
+cudaError_t adjoint_step(vt_ctx* c, const double2* X, double dt) {
+  AdjointState* s = c->adj;
+  AdjArgs a = adj_args(c);
+  cudaError_t e;
+  a.U = s->s3, a.a = s->lam, a.sa = (1.0 / 6) * dt, a.lam = s->lam, a.acc_in = nullptr, a.lam_coef = 1.0;
+  a.acc_out = s->acc, a.a_out = s->a1, a.cl = (1.0 / 3) * dt, a.cg = dt;
+  if ((e = reverse_stage(c, a))) return e;
+  a.U = s->s2, a.a = s->a1, a.sa = 1.0, a.acc_in = s->acc, a.lam_coef = 0.0;
+  a.acc_out = s->acc, a.a_out = s->a0, a.cl = (1.0 / 3) * dt, a.cg = 0.5 * dt;
+  if ((e = reverse_stage(c, a))) return e;
+  a.U = s->s1, a.a = s->a0, a.a_out = s->a1, a.cl = (1.0 / 6) * dt, a.cg = 0.5 * dt;
+  if ((e = reverse_stage(c, a))) return e;
+  a.U = X, a.a = s->a1, a.lam = nullptr, a.acc_out = s->lam, a.a_out = nullptr, a.cl = 0.0, a.cg = 0.0;
+  return reverse_stage(c, a);
+}
+
+// Runs plan[begin, end). `out_last` receives the new state of the plan's first
+// stage step (the forward sweep's last step), or null to skip that stage.
+cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
+  AdjointState* s = c->adj;
+  cudaError_t e = cudaSuccess;
+  for (size_t i = begin; i < end && !e; ++i) {
+    const CkptAction& a = s->plan[i];
+    switch (a.op) {
+      case CkptOp::kAdvance: e = advance(c, slot(c, a.src), a.steps, slot(c, a.dst), s->dt); break;
+      case CkptOp::kStageStep:
+        e = stage_step(c, slot(c, a.src), s->dt, a.step == s->nsteps - 1 ? out_last : nullptr);
+        break;
+      case CkptOp::kAdjoint: e = adjoint_step(c, slot(c, a.src), s->dt); break;
+    }
+  }
+  return e;
+}
+
+// Host or device AoS array -> SoA buffer on the context's stream.
+cudaError_t load_aos(vt_ctx* c, const double* src, int device_pointers, double2* dst) {
+  if (device_pointers) return aos_to_soa(c, src, dst);
+  cudaError_t e = cudaMemcpyAsync(c->aos, src, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np,
+                                  cudaMemcpyHostToDevice, c->stream);
+  return e ? e : aos_to_soa(c, reinterpret_cast<const double*>(c->aos), dst);
+}
+
+cudaError_t store_aos(vt_ctx* c, const double2* src, double* dst, int device_pointers) {
+  if (device_pointers) return soa_to_aos(c, src, dst);
+  cudaError_t e = soa_to_aos(c, src, reinterpret_cast<double*>(c->aos));
+  if (!e)
+    e = cudaMemcpyAsync(dst, c->aos, sizeof(double) * 4 * static_cast<size_t>(c->K) * c->Np, cudaMemcpyDeviceToHost,
+                        c->stream);
+  return e;
+}
+
+cudaError_t lincomb(vt_ctx* c, double2* out, const double2* x, double cx, const double2* y, double cy,
+                    const double2* z = nullptr, double cz = 0.0) {
+  const long long n = static_cast<long long>(c->adj->state_elems);
+  lincomb_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(out, x, cx, y, cy, z, cz, n);
+  return cudaGetLastError();
+}
+
+int prepare(vt_ctx* c) {
+  int st = setup(c);
+  if (!st) st = ensure_aos(c);
+  return st;
+}
+
+}  // namespace
+
+void adjoint_release(vt_ctx* c) {
+  if (!c || !c->adj) return;
+  if (c->adj->slots) cudaFree(c->adj->slots);
+  if (c->adj->bufs) cudaFree(c->adj->bufs);
+  delete c->adj;
+  c->adj = nullptr;
+}
+
+}  // namespace vt
+
+using vt::fail;
+
+extern "C" {
+
+int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
+  if (!c || nsteps < 1 || nsnapshots < 1) return fail(VT_ERR_INVALID, "vt_adjoint_forward: bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
+  int st = vt::prepare(c);
+  if (st) return st;
+  vt::AdjointState* s = c->adj;
+  s->have_forward = s->fresh = false;
+  const int S = std::min(nsnapshots, nsteps);
+  s->plan = vt::plan_reversal(nsteps, S);
+  s->dt = dt;
+  s->nsteps = nsteps;
+  s->first_adjoint = 0;
+  int used = 1;
+  while (s->plan[s->first_adjoint].op != vt::CkptOp::kAdjoint) ++s->first_adjoint;
+  for (const vt::CkptAction& a : s->plan)
+    if (a.op == vt::CkptOp::kAdvance && a.dst != vt::kWorkSlot) used = std::max(used, a.dst + 1);
+  if ((st = vt::ensure_slots(c, used))) return st;
+  if ((st = vt_checkpoint_plan(nsteps, S, &s->info))) return st;
+  cudaError_t e = cudaMemcpyAsync(vt::slot(c, 0), c->U, sizeof(double2) * s->state_elems, cudaMemcpyDeviceToDevice,
+                                  c->stream);
+  if (!e) e = vt::reset_error_words(c);
+  if (!e) e = vt::run_plan(c, 0, s->first_adjoint, c->U);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint forward", e));
+  st = vt::finish(c, nsteps, dt);
+  if (st == VT_OK) s->have_forward = s->fresh = true;
+  return st;
+}
+
+int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int device_pointers) {
+  if (!c || !dJdU_T || !dJdU_0) return fail(VT_ERR_INVALID, "vt_adjoint_backward: null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
+  vt::AdjointState* s = c->adj;
+  if (!s || !s->have_forward) return fail(VT_ERR_INVALID, "vt_adjoint_backward: no forward sweep to reverse");
+  cudaError_t e = vt::reset_error_words(c);
+  // the checkpoints of the forward sweep were reused by an earlier reverse
+  // sweep (or the stage states by other calls): replay the sweep from U_0
+  if (!e && !s->fresh) e = vt::run_plan(c, 0, s->first_adjoint, nullptr);
+  s->fresh = false;
+  if (!e) e = vt::load_aos(c, dJdU_T, device_pointers, s->lam);
+  if (!e) e = vt::run_plan(c, s->first_adjoint, s->plan.size(), nullptr);
+  if (!e) e = vt::store_aos(c, s->lam, dJdU_0, device_pointers);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint backward", e));
+  return vt::finish(c, 0, 0.0);
+}
+
+int vt_adjoint_info(const vt_ctx* c, vt_checkpoint_info* out) {
+  if (!c || !out) return fail(VT_ERR_INVALID, "vt_adjoint_info: null argument");
+  if (!c->adj || !c->adj->have_forward) return fail(VT_ERR_INVALID, "vt_adjoint_info: no forward sweep");
+  *out = c->adj->info;
+  return VT_OK;
+}
+
+int vt_rhs_jvp(vt_ctx* c, const double* U, const double* V, double* dR, int device_pointers) {
+  if (!c || !U || !V || !dR) return fail(VT_ERR_INVALID, "vt_rhs_jvp: null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  int st = vt::prepare(c);
+  if (st) return st;
+  vt::AdjointState* s = c->adj;
+  s->fresh = false;
+  cudaError_t e = vt::load_aos(c, U, device_pointers, s->s1);
+  if (!e) e = vt::load_aos(c, V, device_pointers, s->s2);
+  if (!e) e = s->k.jvp(s->s1, s->s2, s->s3, c->geo, c->nbr, c->Kpad, c->K, c->ops.data(), c->stream);
+  if (!e) e = vt::store_aos(c, s->s3, dR, device_pointers);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("rhs jvp", e)) : VT_OK;
+}
+
+int vt_rhs_vjp(vt_ctx* c, const double* U, const double* W, double* G, int device_pointers) {
+  if (!c || !U || !W || !G) return fail(VT_ERR_INVALID, "vt_rhs_vjp: null argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  int st = vt::prepare(c);
+  if (st) return st;
+  vt::AdjointState* s = c->adj;
+  s->fresh = false;
+  cudaError_t e = vt::load_aos(c, U, device_pointers, s->s1);
+  if (!e) e = vt::load_aos(c, W, device_pointers, s->s2);
+  if (!e) {
+    vt::AdjArgs a = vt::adj_args(c);
+    a.U = s->s1, a.a = s->s2, a.acc_out = s->s3;
+    e = vt::reverse_stage(c, a);
+  }
+  if (!e) e = vt::store_aos(c, s->s3, G, device_pointers);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("rhs vjp", e)) : VT_OK;
+}
+
+int vt_tangent_rk4(vt_ctx* c, double dt, int nsteps, const double* dU_0, double* dU_T, int device_pointers) {
+  if (!c || nsteps < 0 || !dU_0 || !dU_T) return fail(VT_ERR_INVALID, "vt_tangent_rk4: bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
+  int st = vt::prepare(c);
+  if (st) return st;
+  vt::AdjointState* s = c->adj;
+  s->fresh = false;
+  double2 *dX = s->a0, *dS = s->a1, *dacc = s->acc, *dk = s->lam;
+  const double2* X = c->U;
+  auto jvp = [&](const double2* at, const double2* v) {
+    return s->k.jvp(at, v, dk, c->geo, c->nbr, c->Kpad, c->K, c->ops.data(), c->stream);
+  };
+  cudaError_t e = vt::load_aos(c, dU_0, device_pointers, dX);
+  if (!e) e = vt::reset_error_words(c);
+  for (int n = 0; n < nsteps && !e; ++n) {
+    if ((e = vt::stage_step(c, X, dt, nullptr))) break;
+    if ((e = jvp(X, dX)) || (e = vt::lincomb(c, dacc, dX, 1.0, dk, (1.0 / 6) * dt)) ||
+        (e = vt::lincomb(c, dS, dX, 1.0, dk, 0.5 * dt)))
+      break;
+    if ((e = jvp(s->s1, dS)) || (e = vt::lincomb(c, dacc, dacc, 1.0, dk, (1.0 / 3) * dt)) ||
+        (e = vt::lincomb(c, dS, dX, 1.0, dk, 0.5 * dt)))
+      break;
+    if ((e = jvp(s->s2, dS)) || (e = vt::lincomb(c, dacc, dacc, 1.0, dk, (1.0 / 3) * dt)) ||
+        (e = vt::lincomb(c, dS, dX, 1.0, dk, dt)))
+      break;
+    if ((e = jvp(s->s3, dS)) || (e = vt::lincomb(c, dX, dacc, 1.0, dk, (1.0 / 6) * dt))) break;
+    e = vt::stage(c, s->s3, X, c->U, 3, 0.0, (1.0 / 6) * dt);
+  }
+  if (!e) e = vt::store_aos(c, dX, dU_T, device_pointers);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("tangent", e));
+  return vt::finish(c, nsteps, dt);
+}
+
+int vt_roe_flux(const double* uL, const double* uR, double nx, double ny, double* flux) {
+  if (!uL || !uR || !flux) return fail(VT_ERR_INVALID, "vt_roe_flux: null argument");
+  return vt::roe_flux_t(uL, uR, nx, ny, flux);
+}
+
+int vt_roe_flux_jvp(const double* uL, const double* uR, double nx, double ny, const double* duL, const double* duR,
+                    double* dflux) {
+  if (!uL || !uR || !duL || !duR || !dflux) return fail(VT_ERR_INVALID, "vt_roe_flux_jvp: null argument");
+  vt::Dual<1> L[4], R[4], f[4];
+  for (int c = 0; c < 4; ++c) {
+    L[c] = vt::Dual<1>(uL[c]);
+    L[c].d[0] = duL[c];
+    R[c] = vt::Dual<1>(uR[c]);
+    R[c].d[0] = duR[c];
+  }
+  const int code = vt::roe_flux_t(L, R, nx, ny, f);
+  for (int c = 0; c < 4; ++c) dflux[c] = f[c].d[0];
+  return code;
+}
+
+void vt_roe_flux_vjp(const double* uL, const double* uR, double nx, double ny, const double* bflux, double* buL,
+                     double* buR) {
+  if (!uL || !uR || !bflux || !buL || !buR) return;
+  vt::roe_flux_vjp(uL, uR, nx, ny, bflux, buL, buR);
+}
+
+}  // extern "C"

@@ -13,6 +13,7 @@
 
 #include "../../include/vortex_b200.h"
 #include "vt_common.h"
+#include "vt_ctx.h"
 #include "vt_precompute.h"
 #include "vt_launch.h"
 
@@ -129,38 +130,13 @@ __global__ void totals_final_kernel(const double* __restrict__ partial, int nblo
   if (threadIdx.x < 4) out[threadIdx.x] = red[threadIdx.x][0];
 }
 
+}  // namespace
+
 std::string cuda_msg(const char* what, cudaError_t e) {
   return std::string(what) + ": " + cudaGetErrorString(e);
 }
 
-}  // namespace
 }  // namespace vt
-
-struct vt_ctx {
-  std::mutex mu;
-  int device = 0, p = 0, Np = 0, nfq = 0, K = 0;
-  long long Kpad = 0;
-  int max_blocks = 0;  // persistent grid: SMs x resident blocks per SM
-  cudaStream_t stream = nullptr;
-  double2 *U = nullptr, *A = nullptr, *Sa = nullptr, *Sb = nullptr, *R = nullptr;
-  double2* geo = nullptr;
-  int4* nbr = nullptr;
-  int4* tiles = nullptr;     // tile runs
-  int* tile_items = nullptr;  // per-tile face lists
-  int* tile_count = nullptr;
-  int ntiles = 0;
-  unsigned long long* err = nullptr;
-  double2* aos = nullptr;
-  double *W = nullptr, *partial = nullptr, *tot = nullptr;
-  std::vector<double> ops;
-  vt::LaunchFn launch = nullptr;
-  double time = 0.0;
-  cudaGraphExec_t rk4_graph = nullptr;
-  double rk4_graph_dt = 0.0;
-  vt_error_info last{};
-  int pending_steps = 0;
-  double pending_dt = 0.0;
-};
 
 namespace {
 
@@ -174,6 +150,7 @@ cudaError_t alloc(T** p, size_t bytes) {
 void release(vt_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  vt::adjoint_release(c);
   if (c->rk4_graph) cudaGraphExecDestroy(c->rk4_graph);
   void* bufs[] = {c->U,  c->A,     c->Sa,  c->Sb,         c->R,          c->geo,     c->nbr,
                   c->err, c->aos,  c->W,   c->partial,    c->tot,        c->tiles,   c->tile_items,
@@ -183,6 +160,10 @@ void release(vt_ctx* c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
+
+}  // namespace
+
+namespace vt {
 
 vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, double2* acc, double2* out,
                          int stage, double c_acc, double c_out) {
@@ -271,7 +252,15 @@ cudaError_t soa_to_aos(vt_ctx* c, const double2* src, double* dst) {
   return cudaGetLastError();
 }
 
-}  // namespace
+}  // namespace vt
+
+using vt::aos_to_soa;
+using vt::enqueue_rk4_step;
+using vt::ensure_aos;
+using vt::finish;
+using vt::reset_error_words;
+using vt::soa_to_aos;
+using vt::stage_args;
 
 extern "C" {
 
@@ -343,6 +332,13 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
     geo[6 * KP + n] = make_double2(ln[2] / det, det);
     const int right = d->neighbours[3 * n], left = d->neighbours[3 * n + 1], vert = d->neighbours[3 * n + 2];
     nbr[n] = d->element_type[n] == 0 ? make_int4(vert, right, left, 0) : make_int4(vert, left, right, 0);
+  }
+  // side s of an element faces side s of its neighbour (Evolve.cpp:167-202 on
+  // the reference mesh); the adjoint's gather of neighbour face terms needs it
+  c->side_pairing = true;
+  for (int n = 0; n < K && c->side_pairing; ++n) {
+    const int4 b = nbr[n];
+    c->side_pairing = nbr[b.x].x == n && nbr[b.y].y == n && nbr[b.z].z == n;
   }
   // W_i = integral of phi_i = sum_j M_ref[i][j] (the basis sums to one)
   std::vector<double> m(d->inv_mass_ref, d->inv_mass_ref + c->Np * c->Np), W(c->Np, 0.0);
