@@ -236,6 +236,57 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0):
     }
 
 
+def adjoint(vt, steps: int = 2000, snapshots=(45, 2000), device: int = 0):
+    """Adjoint/forward time ratio on the adjoint configuration: the reference
+    vortex on 128x128 cells (32,768 triangles), p=3, io=10, RK4 dt=8.8e-5.
+    forward = `steps` plain RK4 steps (vt_step_rk4); adjoint = forward sweep
+    with checkpoints + reverse sweep (recomputation included) through
+    vt_adjoint_forward/backward, for each checkpoint budget. Device time with
+    CUDA events on the solver's stream, after one untimed run of each."""
+    import numpy as np
+    import torch
+
+    dt = 8.8e-5
+    pb = vt.Problem(vt.make_params(128, 128, p=3, integration_order=10, time_step=dt))
+    s = vt.Solver(pb, device=device)
+    U0 = pb.array("U0")
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", device))
+    lamT = torch.tensor(np.random.default_rng(3).standard_normal(U0.shape), device=torch.device("cuda", device))
+
+    def timed(fn):
+        fn()  # untimed: graph capture, buffers
+        s.upload(U0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def fwd():
+        s.upload(U0)
+        s.rk4(dt, steps)
+
+    fwd_ms = timed(fwd)
+    out = {"workload": f"reference vortex, 128x128 cells (32,768 triangles), p=3, io=10, RK4 dt={dt}, "
+                       f"{steps} steps; J gradient w.r.t. U(0) (1.31M values)",
+           "forward_ms": fwd_ms, "runs": []}
+    for ns in snapshots:
+        def adj(ns=ns):
+            s.upload(U0)
+            s.adjoint_forward(dt, steps, ns)
+            s.adjoint_backward(lamT)
+        ms = timed(adj)
+        info = s.adjoint_info()
+        out["runs"].append({"snapshots": ns, "adjoint_ms": ms, "ratio": ms / fwd_ms,
+                            "state_mb_per_snapshot": U0.nbytes / 1e6,
+                            "advance_steps": info["advance_steps"], "stage_steps": info["stage_steps"],
+                            "optimal_advance_steps": info["optimal_advance_steps"]})
+    s.close()
+    return out
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
