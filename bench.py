@@ -236,12 +236,14 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0):
     }
 
 
-def adjoint(vt, steps: int = 2000, snapshots=(45, 2000), device: int = 0):
+def adjoint(vt, steps: int = 2000, snapshots=(45, 2000, 8000), device: int = 0):
     """Adjoint/forward time ratio on the adjoint configuration: the reference
     vortex on 128x128 cells (32,768 triangles), p=3, io=10, RK4 dt=8.8e-5.
     forward = `steps` plain RK4 steps (vt_step_rk4); adjoint = forward sweep
     with checkpoints + reverse sweep (recomputation included) through
-    vt_adjoint_forward/backward, for each checkpoint budget. Device time with
+    vt_adjoint_forward/backward, for each checkpoint budget: 45 states on the
+    binomial schedule, every step start (2000), and every step start and
+    stage state (8000 states, 84 GB: nothing recomputed). Device time with
     CUDA events on the solver's stream, after one untimed run of each."""
     import numpy as np
     import torch
@@ -282,7 +284,8 @@ def adjoint(vt, steps: int = 2000, snapshots=(45, 2000), device: int = 0):
         out["runs"].append({"snapshots": ns, "adjoint_ms": ms, "ratio": ms / fwd_ms,
                             "state_mb_per_snapshot": U0.nbytes / 1e6,
                             "advance_steps": info["advance_steps"], "stage_steps": info["stage_steps"],
-                            "optimal_advance_steps": info["optimal_advance_steps"]})
+                            "optimal_advance_steps": info["optimal_advance_steps"],
+                            "all_stages": bool(info["all_stages"])})
     s.close()
     return out
 
@@ -409,6 +412,7 @@ def b200_arm(args):
         traffic = profile_traffic()
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
         ens = ensemble(vt, args.ensemble_steps, device=local) if world == 1 and args.ensemble_steps > 0 else None
+        adj = adjoint(vt, args.adjoint_steps, device=local) if world == 1 and args.adjoint_steps > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -431,6 +435,7 @@ def b200_arm(args):
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
             "ensemble": ens,
+            "adjoint": adj,
         }
         print(json.dumps(line))
     solver.close()
@@ -450,6 +455,8 @@ def main():
     ap.add_argument("--cells", type=int, default=NX, help="cells per side (profiling runs use fewer)")
     ap.add_argument("--ensemble-steps", type=int, default=500,
                     help="RK4 steps of the 512-problem ensemble comparison at N=1 (0 skips it)")
+    ap.add_argument("--adjoint-steps", type=int, default=2000,
+                    help="RK4 steps of the adjoint/forward time ratio at N=1 (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

@@ -231,15 +231,19 @@ int vt_batch_set_blocks_per_sm(vt_batch* batch, const int* blocks_per_sm);
  * device memory on the context's device). Needs a mesh whose side s faces its
  * neighbour's side s (the reference mesh does); VT_ERR_UNSUPPORTED otherwise. */
 
-/* Schedule of the binomial checkpointing of an nsteps-step run with
- * `nsnapshots` stored states (U_0 included). */
+/* Schedule of the checkpointing of an nsteps-step run with `nsnapshots`
+ * stored states (U_0 included). With nsnapshots >= 4 nsteps every step's start
+ * and three stage states are kept and nothing is recomputed (all_stages = 1);
+ * otherwise step starts are checkpointed on the binomial schedule and each
+ * step is rerun once, keeping its stage states, before its reverse. */
 typedef struct vt_checkpoint_info {
   int64_t advance_steps;         /* plain RK4 steps, forward sweep included */
-  int64_t forward_sweep_steps;   /* of which in the forward sweep (nsteps - 1) */
-  int64_t stage_steps;           /* steps rerun keeping stage states (= nsteps) */
+  int64_t forward_sweep_steps;   /* of which in the forward sweep */
+  int64_t stage_steps;           /* steps run keeping stage states (= nsteps) */
   int64_t adjoint_steps;         /* = nsteps */
   int64_t optimal_advance_steps; /* Griewank's bound r n - C(S + r, S + 1) */
-  int32_t slots_used;            /* snapshot buffers actually used */
+  int32_t slots_used;            /* state buffers actually used */
+  int32_t all_stages;            /* 1: every stage state kept, no recomputation */
 } vt_checkpoint_info;
 
 /* Plans the reversal on the host only (no device needed). */
@@ -247,7 +251,8 @@ int vt_checkpoint_plan(int nsteps, int nsnapshots, vt_checkpoint_info* out);
 
 /* Forward sweep: nsteps RK4 steps of size dt from the current state, keeping
  * at most `nsnapshots` states in device memory (nsnapshots >= nsteps keeps
- * every step's start). On return the context holds U(T) exactly as
+ * every step's start; >= 4 nsteps also every stage state, so the reverse
+ * sweep recomputes nothing). On return the context holds U(T) exactly as
  * vt_step_rk4 would leave it and the time has advanced; a non-physical state
  * returns its code. */
 int vt_adjoint_forward(vt_ctx* ctx, double dt, int nsteps, int nsnapshots);

@@ -5,8 +5,10 @@
   kernel's right-hand side;
 * over a run, the tangent-linear model and the checkpointed reverse sweep
   satisfy <lam_T, dU_T> = <lam_0, dU_0> to 1e-10, the reverse sweep is bitwise
-  independent of the number of checkpoints, and its forward sweep is bitwise
-  vt_step_rk4;
+  independent of the number of checkpoints (every stage state kept, or step
+  starts on the binomial schedule), and its forward sweep is bitwise
+  vt_step_rk4; the two-sided face phase (meshes that do not 2-colour) obeys
+  the same stage identity as the edge-once one;
 * gradients of the mass-weighted loss J = 1/2 ||U(T) - U*(T)||_M agree with
   finite differences of the forward stepper to 1e-6 relative at h = 1e-4,
   1e-5, 1e-6 (fourth-order differences; central ones at 1e-5 and 1e-6, whose
@@ -88,6 +90,29 @@ def test_rhs_vjp_is_transpose_of_jvp(vt, nx, ny, p, io):
     assert rel(np.sum(W * JV), np.sum(JtW * V)) < 1e-12
 
 
+def test_rhs_vjp_two_sided_faces(vt):
+    """A mesh that does not 2-colour (one element pair made self-neighbours
+    across side 0, which keeps every side paired with itself) takes the
+    two-sided face phase; the transpose identity must hold there too."""
+    pb = problem(vt, 12, 10, 3, 10)
+    conn = pb.array("conn").copy()
+    a = 5
+    b = conn[a, 2]  # side 0 is the vertical neighbour for both element types
+    conn[a, 2], conn[b, 2] = a, b
+    desc = vt.mesh_desc_from_arrays(pb.p, pb.array("type"), conn, pb.array("detj"), pb.array("jinv"),
+                                    pb.array("normals"), pb.array("sides"), pb.array("minv_ref"),
+                                    pb.array("stiff_ref"), pb.array("line_quad"), pb.array("phi_plus"),
+                                    pb.array("phi_minus"))
+    s = vt.Solver(desc)
+    rng = np.random.default_rng(41)
+    U = pb.array("U0")
+    V = rng.standard_normal(U.shape) * state_scale(U)
+    W = rng.standard_normal(U.shape)
+    JV = s.rhs_jvp(U, V)
+    JtW = s.rhs_vjp(U, W)
+    assert rel(np.sum(W * JV), np.sum(JtW * V)) < 1e-12
+
+
 @pytest.mark.parametrize("nx,ny,p,io", [(16, 16, 3, 10), (12, 10, 2, 6)])
 def test_rhs_jvp_matches_central_differences(vt, nx, ny, p, io):
     pb = problem(vt, nx, ny, p, io)
@@ -119,11 +144,12 @@ def test_tangent_adjoint_dot_product_and_checkpoints(vt):
     ref.rk4(dt, n)
     np.testing.assert_array_equal(UT, ref.download())
     lams = []
-    for nsnap in (n, 5, 2, 1):
+    for nsnap in (4 * n, n, 5, 2, 1):
         s.upload(U0)
         s.adjoint_forward(dt, n, nsnap)
         np.testing.assert_array_equal(s.download(), UT)
         info = s.adjoint_info()
+        assert info["all_stages"] == (nsnap >= 4 * n)
         assert info["advance_steps"] == info["optimal_advance_steps"]
         assert info["slots_used"] <= nsnap
         lams.append(s.adjoint_backward(lT))

@@ -89,7 +89,8 @@ class vt_device_mesh(ctypes.Structure):
 class vt_checkpoint_info(ctypes.Structure):
     _fields_ = [("advance_steps", ctypes.c_int64), ("forward_sweep_steps", ctypes.c_int64),
                 ("stage_steps", ctypes.c_int64), ("adjoint_steps", ctypes.c_int64),
-                ("optimal_advance_steps", ctypes.c_int64), ("slots_used", ctypes.c_int32)]
+                ("optimal_advance_steps", ctypes.c_int64), ("slots_used", ctypes.c_int32),
+                ("all_stages", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

@@ -3,10 +3,12 @@
 //
 // Forward sweep: the plain RK4 step (the stage kernel of vt_step_rk4, launched
 // on explicit buffers) advances between checkpoint slots as the binomial plan
-// of vt_checkpoint.h says. Reverse sweep, per step i = n-1 .. 0: rerun step i
-// from its checkpoint keeping the stage states U1, U2, U3, then four reverse
-// stages (adjoint_face_kernel + adjoint_element_kernel each) turn the adjoint
-// of U_{i+1} into the adjoint of U_i:
+// of vt_checkpoint.h says, or, when the snapshot budget holds four states per
+// step, writes every step's start and stage states to their own buffers.
+// Reverse sweep, per step i = n-1 .. 0: (binomial plan) rerun step i from its
+// checkpoint keeping the stage states U1, U2, U3; then four reverse stages (a
+// face phase + adjoint_element_kernel each) turn the adjoint of U_{i+1} into
+// the adjoint of U_i:
 //   a4 = dt/6 lam                 g4 = R'(U3)^T a4
 //   a3 = dt/3 lam + dt   g4       g3 = R'(U2)^T a3
 //   a2 = dt/3 lam + dt/2 g3       g2 = R'(U1)^T a2
@@ -36,6 +38,7 @@ using JvpFn = cudaError_t (*)(const double2*, const double2*, double2*, const do
 
 struct AdjKernels {
   FaceFn face = nullptr;
+  FaceFn edge = nullptr;
   FaceFn element = nullptr;
   JvpFn jvp = nullptr;
 };
@@ -46,6 +49,15 @@ cudaError_t launch_face(const AdjArgs& a, const double* ops, cudaStream_t st) {
   std::memcpy(&o, ops, sizeof(o));
   const dim3 grid((a.K + kAdjRun - 1) / kAdjRun, 3), block(kAdjRun, NFQ);
   adjoint_face_kernel<P, NFQ><<<grid, block, 0, st>>>(a, o);
+  return cudaGetLastError();
+}
+
+template <int P, int NFQ>
+cudaError_t launch_edge(const AdjArgs& a, const double* ops, cudaStream_t st) {
+  StageOps<P, NFQ> o;
+  std::memcpy(&o, ops, sizeof(o));
+  const dim3 grid((a.nowners + kAdjRun - 1) / kAdjRun, 3), block(kAdjRun, NFQ);
+  adjoint_edge_kernel<P, NFQ><<<grid, block, 0, st>>>(a, o);
   return cudaGetLastError();
 }
 
@@ -69,7 +81,7 @@ cudaError_t launch_jvp(const double2* U, const double2* V, double2* dR, const do
 
 template <int P, int NFQ>
 AdjKernels kernels_of() {
-  return AdjKernels{launch_face<P, NFQ>, launch_element<P, NFQ>, launch_jvp<P, NFQ>};
+  return AdjKernels{launch_face<P, NFQ>, launch_edge<P, NFQ>, launch_element<P, NFQ>, launch_jvp<P, NFQ>};
 }
 
 template <int P>
@@ -109,14 +121,19 @@ struct AdjointState {
   double2 *work = nullptr, *s1 = nullptr, *s2 = nullptr, *s3 = nullptr;
   double2 *lam = nullptr, *acc = nullptr, *a0 = nullptr, *a1 = nullptr;
   double2 *bp = nullptr, *bm = nullptr;  // face adjoints
+  // edge-once face phase: owner elements (null when the mesh does not 2-colour)
+  int* owners = nullptr;
+  unsigned char* is_owner = nullptr;
+  int nowners = 0;
   double2* slots = nullptr;
-  int nslots = 0;
+  long long nslots = 0;
   // last forward sweep
   std::vector<CkptAction> plan;
   size_t first_adjoint = 0;
   double dt = 0.0;
   int nsteps = 0;
   bool have_forward = false;
+  bool all_stages = false;  // every step's start and stage states are kept in slots 4i .. 4i+3
   bool fresh = false;  // the forward sweep's checkpoints and stage states are intact
   vt_checkpoint_info info{};
 };
@@ -146,10 +163,51 @@ int setup(vt_ctx* c) {
   s->bp = s->bufs + 8 * s->state_elems;
   s->bm = s->bp + face_elems;
   c->adj = s;
+  // Owners for the edge-once face phase: a 2-colouring of the element
+  // adjacency (breadth first); colour 0 owns every edge it touches.
+  std::vector<int4> nb(static_cast<size_t>(c->K));
+  e = cudaMemcpy(nb.data(), c->nbr, sizeof(int4) * nb.size(), cudaMemcpyDeviceToHost);
+  if (e) return fail(VT_ERR_CUDA, cuda_msg("adjoint: neighbours", e));
+  std::vector<signed char> col(nb.size(), -1);
+  std::vector<int> queue;
+  bool ok = true;
+  for (int start = 0; start < c->K && ok; ++start) {
+    if (col[start] >= 0) continue;
+    col[start] = 0;
+    queue.assign(1, start);
+    for (size_t h = 0; h < queue.size() && ok; ++h) {
+      const int x = queue[h];
+      const int side[3] = {nb[x].x, nb[x].y, nb[x].z};
+      for (int n : side) {
+        if (col[n] < 0) {
+          col[n] = static_cast<signed char>(1 - col[x]);
+          queue.push_back(n);
+        } else if (col[n] == col[x]) {
+          ok = false;
+        }
+      }
+    }
+  }
+  if (ok) {
+    std::vector<int> owners;
+    std::vector<unsigned char> flag(nb.size());
+    for (int x = 0; x < c->K; ++x) {
+      flag[x] = col[x] == 0;
+      if (flag[x]) owners.push_back(x);
+    }
+    s->nowners = static_cast<int>(owners.size());
+    e = cudaMalloc(reinterpret_cast<void**>(&s->owners), sizeof(int) * owners.size() + flag.size());
+    if (!e) {
+      s->is_owner = reinterpret_cast<unsigned char*>(s->owners + owners.size());
+      e = cudaMemcpy(s->owners, owners.data(), sizeof(int) * owners.size(), cudaMemcpyHostToDevice);
+    }
+    if (!e) e = cudaMemcpy(s->is_owner, flag.data(), flag.size(), cudaMemcpyHostToDevice);
+    if (e) return fail(VT_ERR_CUDA, cuda_msg("adjoint: owners", e));
+  }
   return VT_OK;
 }
 
-int ensure_slots(vt_ctx* c, int n) {
+int ensure_slots(vt_ctx* c, long long n) {
   AdjointState* s = c->adj;
   if (s->nslots >= n) return VT_OK;
   if (s->slots) cudaFree(s->slots);
@@ -165,7 +223,7 @@ int ensure_slots(vt_ctx* c, int n) {
   return VT_OK;
 }
 
-double2* slot(vt_ctx* c, int i) {
+double2* slot(vt_ctx* c, long long i) {
   return i == kWorkSlot ? c->adj->work : c->adj->slots + static_cast<size_t>(i) * c->adj->state_elems;
 }
 
@@ -188,21 +246,28 @@ cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt) {
   return e;
 }
 
-// Step from X keeping the stage states in s1, s2, s3; the new state goes to
+// Step from X keeping the stage states in S1, S2, S3; the new state goes to
 // `out` when given (else the last stage is not run).
-cudaError_t stage_step(vt_ctx* c, const double2* X, double dt, double2* out) {
-  AdjointState* s = c->adj;
+cudaError_t stage_step(vt_ctx* c, const double2* X, double2* S1, double2* S2, double2* S3, double dt,
+                       double2* out) {
   cudaError_t e;
-  if ((e = stage(c, X, X, s->s1, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
-  if ((e = stage(c, s->s1, X, s->s2, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
-  if ((e = stage(c, s->s2, X, s->s3, 2, (1.0 / 3) * dt, dt))) return e;
-  return out ? stage(c, s->s3, X, out, 3, 0.0, (1.0 / 6) * dt) : cudaSuccess;
+  if ((e = stage(c, X, X, S1, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
+  if ((e = stage(c, S1, X, S2, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
+  if ((e = stage(c, S2, X, S3, 2, (1.0 / 3) * dt, dt))) return e;
+  return out ? stage(c, S3, X, out, 3, 0.0, (1.0 / 6) * dt) : cudaSuccess;
+}
+
+cudaError_t stage_step(vt_ctx* c, const double2* X, double dt, double2* out) {
+  return stage_step(c, X, c->adj->s1, c->adj->s2, c->adj->s3, dt, out);
 }
 
 AdjArgs adj_args(vt_ctx* c) {
   AdjArgs a{};
   a.bp = c->adj->bp;
   a.bm = c->adj->bm;
+  a.owners = c->adj->owners;
+  a.is_owner = c->adj->is_owner;
+  a.nowners = c->adj->nowners;
   a.geo = c->geo;
   a.nbr = c->nbr;
   a.Kpad = c->Kpad;
@@ -212,22 +277,23 @@ AdjArgs adj_args(vt_ctx* c) {
 }
 
 cudaError_t reverse_stage(vt_ctx* c, const AdjArgs& a) {
-  cudaError_t e = c->adj->k.face(a, c->ops.data(), c->stream);
+  cudaError_t e = a.is_owner ? c->adj->k.edge(a, c->ops.data(), c->stream) : c->adj->k.face(a, c->ops.data(), c->stream);
   return e ? e : c->adj->k.element(a, c->ops.data(), c->stream);
 }
 
-// lam <- adjoint of U_i given lam = adjoint of U_{i+1}; X = U_i, stage states in s1..s3.
-cudaError_t adjoint_step(vt_ctx* c, const double2* X, double dt) {
+// lam <- adjoint of U_i given lam = adjoint of U_{i+1}; X = U_i, stage states S1..S3.
+cudaError_t adjoint_step(vt_ctx* c, const double2* X, const double2* S1, const double2* S2, const double2* S3,
+                         double dt) {
   AdjointState* s = c->adj;
   AdjArgs a = adj_args(c);
   cudaError_t e;
-  a.U = s->s3, a.a = s->lam, a.sa = (1.0 / 6) * dt, a.lam = s->lam, a.acc_in = nullptr, a.lam_coef = 1.0;
+  a.U = S3, a.a = s->lam, a.sa = (1.0 / 6) * dt, a.lam = s->lam, a.acc_in = nullptr, a.lam_coef = 1.0;
   a.acc_out = s->acc, a.a_out = s->a1, a.cl = (1.0 / 3) * dt, a.cg = dt;
   if ((e = reverse_stage(c, a))) return e;
-  a.U = s->s2, a.a = s->a1, a.sa = 1.0, a.acc_in = s->acc, a.lam_coef = 0.0;
+  a.U = S2, a.a = s->a1, a.sa = 1.0, a.acc_in = s->acc, a.lam_coef = 0.0;
   a.acc_out = s->acc, a.a_out = s->a0, a.cl = (1.0 / 3) * dt, a.cg = 0.5 * dt;
   if ((e = reverse_stage(c, a))) return e;
-  a.U = s->s1, a.a = s->a0, a.a_out = s->a1, a.cl = (1.0 / 6) * dt, a.cg = 0.5 * dt;
+  a.U = S1, a.a = s->a0, a.a_out = s->a1, a.cl = (1.0 / 6) * dt, a.cg = 0.5 * dt;
   if ((e = reverse_stage(c, a))) return e;
   a.U = X, a.a = s->a1, a.lam = nullptr, a.acc_out = s->lam, a.a_out = nullptr, a.cl = 0.0, a.cg = 0.0;
   return reverse_stage(c, a);
@@ -245,7 +311,7 @@ cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
       case CkptOp::kStageStep:
         e = stage_step(c, slot(c, a.src), s->dt, a.step == s->nsteps - 1 ? out_last : nullptr);
         break;
-      case CkptOp::kAdjoint: e = adjoint_step(c, slot(c, a.src), s->dt); break;
+      case CkptOp::kAdjoint: e = adjoint_step(c, slot(c, a.src), s->s1, s->s2, s->s3, s->dt); break;
     }
   }
   return e;
@@ -285,6 +351,7 @@ int prepare(vt_ctx* c) {
 
 void adjoint_release(vt_ctx* c) {
   if (!c || !c->adj) return;
+  if (c->adj->owners) cudaFree(c->adj->owners);
   if (c->adj->slots) cudaFree(c->adj->slots);
   if (c->adj->bufs) cudaFree(c->adj->bufs);
   delete c->adj;
@@ -306,10 +373,30 @@ int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
   if (st) return st;
   vt::AdjointState* s = c->adj;
   s->have_forward = s->fresh = false;
-  const int S = std::min(nsnapshots, nsteps);
-  s->plan = vt::plan_reversal(nsteps, S);
   s->dt = dt;
   s->nsteps = nsteps;
+  s->all_stages = static_cast<long long>(nsnapshots) >= 4ll * nsteps;
+  if (s->all_stages) {
+    // slots 4i .. 4i+3: U_i and the stage states of step i; U_n goes to U
+    if ((st = vt::ensure_slots(c, 4ll * nsteps))) return st;
+    s->plan.clear();
+    s->info = vt_checkpoint_info{};
+    s->info.stage_steps = s->info.adjoint_steps = nsteps;
+    s->info.slots_used = 4 * nsteps;
+    s->info.all_stages = 1;
+    cudaError_t e = cudaMemcpyAsync(vt::slot(c, 0), c->U, sizeof(double2) * s->state_elems,
+                                    cudaMemcpyDeviceToDevice, c->stream);
+    if (!e) e = vt::reset_error_words(c);
+    for (int i = 0; i < nsteps && !e; ++i)
+      e = vt::stage_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
+                         vt::slot(c, 4ll * i + 3), dt, i + 1 < nsteps ? vt::slot(c, 4ll * i + 4) : c->U);
+    if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint forward", e));
+    st = vt::finish(c, nsteps, dt);
+    if (st == VT_OK) s->have_forward = s->fresh = true;
+    return st;
+  }
+  const int S = std::min(nsnapshots, nsteps);
+  s->plan = vt::plan_reversal(nsteps, S);
   s->first_adjoint = 0;
   int used = 1;
   while (s->plan[s->first_adjoint].op != vt::CkptOp::kAdjoint) ++s->first_adjoint;
@@ -335,6 +422,15 @@ int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int dev
   vt::AdjointState* s = c->adj;
   if (!s || !s->have_forward) return fail(VT_ERR_INVALID, "vt_adjoint_backward: no forward sweep to reverse");
   cudaError_t e = vt::reset_error_words(c);
+  if (s->all_stages) {  // nothing to recompute
+    if (!e) e = vt::load_aos(c, dJdU_T, device_pointers, s->lam);
+    for (int i = s->nsteps - 1; i >= 0 && !e; --i)
+      e = vt::adjoint_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
+                           vt::slot(c, 4ll * i + 3), s->dt);
+    if (!e) e = vt::store_aos(c, s->lam, dJdU_0, device_pointers);
+    if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint backward", e));
+    return vt::finish(c, 0, 0.0);
+  }
   // the checkpoints of the forward sweep were reused by an earlier reverse
   // sweep (or the stage states by other calls): replay the sweep from U_0
   if (!e && !s->fresh) e = vt::run_plan(c, 0, s->first_adjoint, nullptr);
