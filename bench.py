@@ -236,15 +236,17 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0):
     }
 
 
-def adjoint(vt, steps: int = 2000, snapshots=(45, 2000, 8000), device: int = 0):
+def adjoint(vt, steps: int = 2000, snapshots=None, device: int = 0):
     """Adjoint/forward time ratio on the adjoint configuration: the reference
     vortex on 128x128 cells (32,768 triangles), p=3, io=10, RK4 dt=8.8e-5.
     forward = `steps` plain RK4 steps (vt_step_rk4); adjoint = forward sweep
     with checkpoints + reverse sweep (recomputation included) through
-    vt_adjoint_forward/backward, for each checkpoint budget: 45 states on the
-    binomial schedule, every step start (2000), and every step start and
-    stage state (8000 states, 84 GB: nothing recomputed). Device time with
-    CUDA events on the solver's stream, after one untimed run of each."""
+    vt_adjoint_forward/backward, for each checkpoint budget (default: 45
+    states on the binomial schedule, every step start, and every step start
+    and stage state, 4 x steps states = 84 GB at 2000 steps: nothing
+    recomputed). Device time with CUDA events on the solver's stream, after
+    one untimed run of each."""
+    snapshots = snapshots or (45, steps, 4 * steps)
     import numpy as np
     import torch
 
