@@ -292,6 +292,42 @@ def adjoint(vt, steps: int = 2000, snapshots=None, device: int = 0):
     return out
 
 
+def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0):
+    """The batched adjoint inverse problem: n vortices on 64x64 cells (8,192
+    triangles), p=2, 300 RK4 steps; seeded true (eps, M, x0, y0) and a
+    perturbed guess; per-instance L-BFGS on the host with every loss
+    evaluation one batched forward + reverse sweep (every step start kept).
+    The time step is the ensemble's stability rule at the lowest Mach number
+    the search may try (0.25): 3.65e-5 (1.5e-4 blows up there, as it does in
+    the reference: the Roe dissipation speed is c^4 = M^-4 = 256)."""
+    import numpy as np
+    from vortex_transport_b200 import inverse, workloads
+
+    theta = inverse.true_parameters(n, seed=5)
+    guess = inverse.perturbed_guess(theta, seed=6)
+    dt = workloads.stable_dt(64, 2, float(inverse.LOWER[1]))
+    t0 = time.perf_counter()
+    inv = inverse.BatchedInverse(theta, side=64, p=2, steps=300, dt=dt, device=device)
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    x, f, done = inv.solve(guess, iterations=iterations)
+    solve_s = time.perf_counter() - t0
+    err0 = np.abs(guess - theta)
+    err = np.abs(x - theta)
+    out = {"workload": f"{n} vortices, 64x64 cells (8,192 triangles) each, p=2, io=10, 300 RK4 steps at "
+                       f"dt={dt:.4g}; true eps~U[0.15,0.45], M~U[0.3,0.6], centre~U[-1.5,1.5]^2 (seed 5); "
+                       "guess eps/M +-0.05, centre +-0.3 (seed 6)",
+           "iterations_max": iterations, "accepted_steps_median": float(np.median(done)),
+           "evaluations": inv.evaluations, "solve_s": solve_s, "s_per_evaluation": solve_s / inv.evaluations,
+           "setup_s": setup_s, "max_param_error_initial": float(err0.max()),
+           "max_param_error_final": float(err.max()),
+           "median_param_error_final": float(np.median(err.max(axis=1))),
+           "loss_reduction_worst": float((f / np.maximum(inv.loss_and_grad(guess)[0], 1e-300)).max()),
+           "checkpoints": inv.batch.adjoint_info()}
+    inv.close()
+    return out
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -415,6 +451,7 @@ def b200_arm(args):
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
         ens = ensemble(vt, args.ensemble_steps, device=local) if world == 1 and args.ensemble_steps > 0 else None
         adj = adjoint(vt, args.adjoint_steps, device=local) if world == 1 and args.adjoint_steps > 0 else None
+        inv = inverse_problem(vt, args.inverse_iters, device=local) if world == 1 and args.inverse_iters > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -438,6 +475,7 @@ def b200_arm(args):
             "clocks": clk.summary(),
             "ensemble": ens,
             "adjoint": adj,
+            "inverse": inv,
         }
         print(json.dumps(line))
     solver.close()
@@ -459,6 +497,9 @@ def main():
                     help="RK4 steps of the 512-problem ensemble comparison at N=1 (0 skips it)")
     ap.add_argument("--adjoint-steps", type=int, default=2000,
                     help="RK4 steps of the adjoint/forward time ratio at N=1 (0 skips it)")
+    ap.add_argument("--inverse-iters", type=int, default=0,
+                    help="L-BFGS iterations of the 128-vortex batched inverse problem at N=1 (0 skips it; "
+                         "50 takes a few minutes)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

@@ -179,6 +179,9 @@ _SIGNATURES = {
     "vt_roe_flux": (ctypes.c_int, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp]),
     "vt_roe_flux_jvp": (ctypes.c_int, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]),
     "vt_roe_flux_vjp": (None, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]),
+    "vt_batch_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "vt_batch_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "vt_batch_adjoint_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "vt_noalloc_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     "vt_step_rk4_noalloc": (ctypes.c_int, [ctypes.POINTER(vt_device_mesh), ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
@@ -624,8 +627,7 @@ class Batch:
         assert dt.shape == (self.n,)
         _check(lib().vt_batch_set_dt(self._h, _ptr(dt)))
 
-    def rk4(self, nsteps: int) -> None:
-        st = lib().vt_batch_step_rk4(self._h, int(nsteps))
+    def _status(self, st: int) -> None:
         if st in (VT_ERR_NONPHYSICAL_LEFT, VT_ERR_NONPHYSICAL_RIGHT, VT_ERR_NONPHYSICAL_C2):
             info, inst = vt_error_info(), ctypes.c_int(-1)
             lib().vt_batch_last_error(self._h, ctypes.byref(inst), ctypes.byref(info))
@@ -633,6 +635,32 @@ class Batch:
             err.instance = inst.value
             raise err
         _check(st)
+
+    def rk4(self, nsteps: int) -> None:
+        self._status(lib().vt_batch_step_rk4(self._h, int(nsteps)))
+
+    # adjoint ----------------------------------------------------------------
+    def adjoint_forward(self, nsteps: int, nsnapshots: int) -> None:
+        """nsteps RK4 steps of every instance keeping checkpoints (the instances
+        of a group share one time step)."""
+        self._status(lib().vt_batch_adjoint_forward(self._h, int(nsteps), int(nsnapshots)))
+
+    def adjoint_backward(self, dJdU_T) -> list[np.ndarray]:
+        """dJ/dU(0) per instance from dJ/dU(T) per instance (lists of (K_i, Np_i, 4))."""
+        flat = np.concatenate([np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in dJdU_T])
+        assert flat.size == sum(K * Np * 4 for K, Np in self.shapes)
+        out = np.empty_like(flat)
+        _check(lib().vt_batch_adjoint_backward(self._h, _ptr(flat), _ptr(out)))
+        res, o = [], 0
+        for K, Np in self.shapes:
+            res.append(out[o:o + K * Np * 4].reshape(K, Np, 4))
+            o += K * Np * 4
+        return res
+
+    def adjoint_info(self, group: int = 0) -> dict:
+        info = vt_checkpoint_info()
+        _check(lib().vt_batch_adjoint_info(self._h, int(group), ctypes.byref(info)))
+        return info.as_dict()
 
     def autotune(self, trials: int = 3, cache: str | None = None) -> list[int]:
         """Resident blocks per SM for each group, tuned on the device and cached

@@ -23,13 +23,12 @@
 
 #include "../../include/vortex_b200.h"
 #include "vt_common.h"
+#include "vt_ctx.h"
 #include "vt_launch.h"
 #include "vt_precompute.h"
 
 namespace vt {
 namespace {
-
-std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
 
 template <typename T>
 cudaError_t dalloc(T** p, size_t bytes) {
@@ -127,6 +126,8 @@ struct vt_batch {
   std::vector<double> dt;  // per instance
   int last_instance = -1;
   vt_error_info last{};
+  // one solver context per group over the group's own buffers, for the adjoint
+  std::vector<vt_ctx*> views;
 };
 
 namespace {
@@ -136,6 +137,11 @@ using vt::fail;
 void release(vt_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
+  for (vt_ctx* v : b->views) {
+    vt::adjoint_release(v);
+    if (v->aos) cudaFree(v->aos);
+    delete v;
+  }
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (auto& g : b->groups) {
     void* bufs[] = {g.U, g.A, g.Sa, g.Sb, g.geo, g.nbr, g.tiles, g.items, g.count, g.tile_dt, g.err};
@@ -223,6 +229,51 @@ int upload_dt(vt_batch* b) {
         cudaMemcpyAsync(g.tile_dt, tdt.data(), sizeof(double) * g.ntiles, cudaMemcpyHostToDevice, b->stream);
     if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("batch dt", e));
     if ((e = cudaStreamSynchronize(b->stream))) return fail(VT_ERR_CUDA, vt::cuda_msg("batch dt", e));
+  }
+  return VT_OK;
+}
+
+// A vt_ctx over a group's buffers (not owning them), so the single-problem
+// adjoint runs on the group's ragged element array: one launch per stage for
+// all its instances. The group's tiles and face lists are the ones the batch
+// steps with; the time step is uniform within the group.
+int ensure_views(vt_batch* b) {
+  if (b->views.size() == b->groups.size()) return VT_OK;
+  for (size_t gi = b->views.size(); gi < b->groups.size(); ++gi) {
+    vt::Group& G = b->groups[gi];
+    auto* c = new vt_ctx();
+    c->device = b->device;
+    c->p = G.p;
+    c->Np = G.Np;
+    c->nfq = G.nfq;
+    c->K = static_cast<int>(G.K);
+    c->Kpad = G.Kpad;
+    c->max_blocks = G.max_blocks;
+    c->stream = b->stream;
+    c->U = G.U;
+    c->A = G.A;
+    c->Sa = G.Sa;
+    c->Sb = G.Sb;
+    c->geo = G.geo;
+    c->nbr = G.nbr;
+    c->tiles = G.tiles;
+    c->tile_items = G.items;
+    c->tile_count = G.count;
+    c->ntiles = G.ntiles;
+    c->err = G.err;
+    c->ops = G.ops;
+    c->launch = G.kern.launch;
+    std::vector<int4> nb(static_cast<size_t>(G.K));
+    const cudaError_t e = cudaMemcpy(nb.data(), G.nbr, sizeof(int4) * nb.size(), cudaMemcpyDeviceToHost);
+    if (e) {
+      delete c;
+      return fail(VT_ERR_CUDA, vt::cuda_msg("batch adjoint set-up", e));
+    }
+    c->side_pairing = true;
+    for (size_t n = 0; n < nb.size() && c->side_pairing; ++n)
+      c->side_pairing = nb[nb[n].x].x == static_cast<int>(n) && nb[nb[n].y].y == static_cast<int>(n) &&
+                        nb[nb[n].z].z == static_cast<int>(n);
+    b->views.push_back(c);
   }
   return VT_OK;
 }
@@ -480,6 +531,73 @@ int vt_batch_step_rk4(vt_batch* b, int nsteps) {
   if (b->last_instance < 0) return VT_OK;
   return fail(b->last.code, "Non-physical state (code " + std::to_string(b->last.code) + ") in instance " +
                                 std::to_string(b->last_instance) + " at element " + std::to_string(b->last.element));
+}
+
+int vt_batch_adjoint_forward(vt_batch* b, int nsteps, int nsnapshots) {
+  if (!b || nsteps < 1 || nsnapshots < 1) return fail(VT_ERR_INVALID, "vt_batch_adjoint_forward: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  int st = ensure_views(b);
+  if (st) return st;
+  b->last = vt_error_info{};
+  b->last_instance = -1;
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    vt::Group& G = b->groups[gi];
+    const double dt = b->dt[G.members[0]];
+    for (int m : G.members)
+      if (b->dt[m] != dt)
+        return fail(VT_ERR_UNSUPPORTED, "vt_batch_adjoint_forward: the instances of a group need one time step");
+    vt_ctx* c = b->views[gi];
+    c->max_blocks = G.max_blocks;
+    st = vt_adjoint_forward(c, dt, nsteps, nsnapshots);
+    if (st > 0) {  // map the group element to its instance
+      vt_error_info info{};
+      vt_last_error(c, &info);
+      const size_t m = std::upper_bound(G.offset.begin(), G.offset.end(), static_cast<long long>(info.element)) -
+                       G.offset.begin() - 1;
+      info.element -= static_cast<int>(G.offset[m]);
+      b->last = info;
+      b->last_instance = G.members[m];
+      return fail(st, "Non-physical state (code " + std::to_string(st) + ") in instance " +
+                          std::to_string(b->last_instance) + " at element " + std::to_string(info.element));
+    }
+    if (st) return st;
+  }
+  return VT_OK;
+}
+
+int vt_batch_adjoint_backward(vt_batch* b, const double* dJdU_T, double* dJdU_0) {
+  if (!b || !dJdU_T || !dJdU_0) return fail(VT_ERR_INVALID, "vt_batch_adjoint_backward: null argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  if (b->views.size() != b->groups.size()) return fail(VT_ERR_INVALID, "vt_batch_adjoint_backward: no forward sweep");
+  std::vector<size_t> off(b->n + 1, 0);  // instance offsets in the concatenated arrays (doubles)
+  for (int i = 0; i < b->n; ++i)
+    off[i + 1] = off[i] + 4 * static_cast<size_t>(b->K_of[i]) * b->groups[b->group_of[i]].Np;
+  std::vector<double> gin, gout;
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    vt::Group& G = b->groups[gi];
+    const size_t per = 4 * static_cast<size_t>(G.Np);
+    gin.resize(per * G.K);
+    gout.resize(per * G.K);
+    for (size_t m = 0; m < G.members.size(); ++m) {
+      const int i = G.members[m];
+      std::memcpy(gin.data() + per * G.offset[m], dJdU_T + off[i], sizeof(double) * (off[i + 1] - off[i]));
+    }
+    const int st = vt_adjoint_backward(b->views[gi], gin.data(), gout.data(), 0);
+    if (st) return st;
+    for (size_t m = 0; m < G.members.size(); ++m) {
+      const int i = G.members[m];
+      std::memcpy(dJdU_0 + off[i], gout.data() + per * G.offset[m], sizeof(double) * (off[i + 1] - off[i]));
+    }
+  }
+  return VT_OK;
+}
+
+int vt_batch_adjoint_info(const vt_batch* b, int group, vt_checkpoint_info* out) {
+  if (!b || !out || group < 0 || group >= static_cast<int>(b->views.size()))
+    return fail(VT_ERR_INVALID, "vt_batch_adjoint_info: bad argument");
+  return vt_adjoint_info(b->views[group], out);
 }
 
 int vt_batch_last_error(const vt_batch* b, int* instance, vt_error_info* out) {
