@@ -97,6 +97,12 @@ int vt_problem_get_info(const vt_problem* prob, vt_problem_info* out);
  * detjinv, normals, sides, U0, F0. */
 int vt_problem_get_array(const vt_problem* prob, const char* name, void* dst, size_t bytes);
 
+/* The exactly translated vortex at time t at the problem's nodes (K x Np x 4):
+ * the initial condition's formula (Element.cpp:134-179) with the centre moved
+ * by (U_infty, V_infty) t and taken as each node's nearest periodic image (the
+ * reference's formula does not wrap). */
+int vt_problem_exact_state(const vt_problem* prob, double t, double* U);
+
 /* Nodal flux of a state, the formula the reference applies after every stage
  * (Timestepping.cpp:141-158). U: K x Np x 4 -> F: K x Np x 2 x 4. */
 int vt_flux_from_state(int K, int p, const double* U, double* F);
@@ -179,6 +185,28 @@ int vt_set_time(vt_ctx* ctx, double t);
 /* Conservation totals sum_e detJ_e sum_i W_i U_e,i (W_i = integral of the
  * i-th basis function), computed on the device. out[4]. */
 int vt_totals(vt_ctx* ctx, double* out);
+
+/* The L2 difference between the current state and U_ref (K x Np x 4, host or
+ * device memory), in the form of the reference's post-processing script
+ * (plottools/l2stateerror.py:65-98): squared nodal differences interpolated
+ * with the basis at the area-rule points area_quad (nq x 3: xi, eta, weight),
+ * integrated with det J, then sqrt(integral / 25) per component; out[4].
+ * Computed on the device. */
+int vt_l2_error(vt_ctx* ctx, int nq, const double* area_quad, const double* U_ref, int device_pointers,
+                double* out);
+
+/* Full-precision dump and restart, replacing the reference's 6-decimal
+ * per-element text dumps (Element::write_data, Element.cpp:336-425) where a
+ * run must resume exactly. A state file is "VTSTATE" + NUL, int32 version (1),
+ * p, K, Np, float64 time, then K x Np x 4 float64 in the reference's U layout.
+ * vt_save_state writes the context's state and time; vt_load_state restores
+ * them (the file must match the context's p and K). The file functions below
+ * need no GPU. */
+int vt_save_state(vt_ctx* ctx, const char* path);
+int vt_load_state(vt_ctx* ctx, const char* path);
+int vt_write_state_file(const char* path, int p, int n_elements, double time, const double* U);
+int vt_state_file_info(const char* path, int* p, int* n_elements, double* time);
+int vt_read_state_file(const char* path, double* U);
 
 /* The context's cudaStream_t, for callers that interleave their own work. */
 void* vt_stream(vt_ctx* ctx);

@@ -1,0 +1,61 @@
+"""The L2 error as a device reduction (vt_l2_error), against the oracle's
+restatement of the reference's post-processing script, and config 1's L2 error
+against the exactly translated vortex after one diagonal transit."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from test_gpu_parity import problem_for
+
+pytestmark = pytest.mark.gpu
+
+# The reference's own script output for the shipped run (io=6, from its
+# 6-decimal text dumps): rho, rho u, rho v, rho E.
+REFERENCE_L2 = [4.694e-5, 4.805e-4, 5.338e-4, 8.084e-4]
+
+
+def basis_at(nodes_ref, p, pts):
+    """Lagrange basis of the reference nodes at pts, from the monomial
+    Vandermonde matrix (an independent evaluation of the basis)."""
+    mon = [(a, b) for a in range(p + 1) for b in range(p + 1 - a)]
+
+    def V(x):
+        return np.stack([x[:, 0] ** a * x[:, 1] ** b for a, b in mon], axis=1)
+
+    return V(pts) @ np.linalg.inv(V(nodes_ref))
+
+
+def oracle_l2(pb, Ua, Ub):
+    import vt_oracle
+    aq = pb.array("area_quad")
+    bq = basis_at(pb.array("nodes_ref"), pb.p, aq[:, :2])
+    return vt_oracle.l2_state_error(bq, aq, pb.array("detj"), Ua, Ub)
+
+
+@pytest.mark.parametrize("p,io", [(3, 10), (2, 8), (1, 6)])
+def test_l2_error_matches_oracle(vt, p, io):
+    pb = vt.Problem(vt.make_params(16, 12, p=p, integration_order=io, perturb_grid=0.2),
+                    vt.vortex(epsilon=0.25, x0=0.7, y0=-0.4))
+    s = vt.Solver(pb)
+    s.rk4(2e-3, 5)
+    U = s.download()
+    rng = np.random.default_rng(p)
+    R = U + 1e-3 * rng.standard_normal(U.shape)
+    got = s.l2_error(R, pb.array("area_quad"))
+    np.testing.assert_allclose(got, oracle_l2(pb, R, U), rtol=1e-12)
+
+
+def test_config1_l2_against_translated_vortex(vt):
+    """After T = 10 sqrt(2) the vortex has crossed the periodic domain once
+    along the diagonal; the exact state is the initial one moved by (10, 10)."""
+    g = golden("c1_p3_io10_rk4_10000")
+    pb = problem_for(vt, g)
+    T = g.meta["dt"] * 10000
+    exact = pb.exact_state(T)
+    np.testing.assert_allclose(exact, pb.array("U0"), rtol=0, atol=5e-6)  # boundary images, see the CPU test
+    s = vt.Solver(pb)
+    s.rk4(g.meta["dt"], 10000)
+    got = s.l2_error(exact, pb.array("area_quad"))
+    np.testing.assert_allclose(got, oracle_l2(pb, exact, s.download()), rtol=1e-12)
+    print("config 1 L2 error vs the translated vortex:", got, "reference script (io=6):", REFERENCE_L2)
+    assert np.all(got < 10 * np.array(REFERENCE_L2))

@@ -123,3 +123,21 @@ def test_parameterised_vortex_reduces_to_reference(vt):
     c = vt.Problem(prm, vt.vortex(epsilon=0.35, M_infty=0.4, x0=0.4, y0=-0.25)).array("U0")
     assert not np.array_equal(a, c)
     assert np.all(c[..., 0] > 0)
+
+
+def test_exact_state_at_time_zero_is_the_initial_condition(vt):
+    """The translated vortex at t = 0 is the nodal initial condition, bit for bit,
+    and one diagonal transit of the periodic domain brings it back. The
+    reference's formula is not periodic (v - V = f2 (x - x0) differs at x = +-5 by
+    ~ 5 exp(-12)), so nodes on the domain boundary, half a period from the
+    centre, may take the other image: 3e-6 there, nothing elsewhere."""
+    prm = vt.make_params(8, 8, p=3, integration_order=10)
+    pb = vt.Problem(prm)
+    np.testing.assert_array_equal(pb.exact_state(0.0), pb.array("U0"))
+    back = pb.exact_state(10 * np.sqrt(2))
+    np.testing.assert_allclose(back, pb.array("U0"), rtol=0, atol=5e-6)
+    X = pb.array("nodes_phys")
+    inner = (np.abs(X[..., 0]) < 4.99) & (np.abs(X[..., 1]) < 4.99)
+    np.testing.assert_allclose(back[inner], pb.array("U0")[inner], rtol=0, atol=1e-12)
+    shifted = pb.exact_state(2.5 * np.sqrt(2))  # centre moved by (2.5, 2.5)
+    assert abs(shifted - pb.array("U0")).max() > 1e-2

@@ -167,6 +167,14 @@ _SIGNATURES = {
     "vt_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "vt_batch_set_blocks_per_sm": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "vt_checkpoint_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "vt_save_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "vt_load_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "vt_write_state_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
+    "vt_state_file_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    "vt_read_state_file": (ctypes.c_int, [ctypes.c_char_p, _dp]),
+    "vt_l2_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_void_p, ctypes.c_int, _dp]),
+    "vt_problem_exact_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp]),
     "vt_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
     "vt_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "vt_adjoint_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -296,6 +304,22 @@ def _is_cuda_tensor(x) -> bool:
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
 
 
+def write_state_file(path: str, p: int, U: np.ndarray, time: float = 0.0) -> None:
+    """Full-precision state file (the format of vt_save_state); no GPU needed."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    _check(lib().vt_write_state_file(os.fsencode(path), int(p), U.shape[0], float(time), _ptr(U)))
+
+
+def read_state_file(path: str):
+    """(U, p, time) from a state file; no GPU needed."""
+    p, K, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    _check(lib().vt_state_file_info(os.fsencode(path), ctypes.byref(p), ctypes.byref(K), ctypes.byref(t)))
+    Np = (p.value + 1) * (p.value + 2) // 2
+    U = np.empty((K.value, Np, 4))
+    _check(lib().vt_read_state_file(os.fsencode(path), _ptr(U)))
+    return U, p.value, t.value
+
+
 def checkpoint_plan(nsteps: int, nsnapshots: int) -> dict:
     """Schedule of the binomial checkpointing of an nsteps-step adjoint run
     with nsnapshots stored states (host only)."""
@@ -366,6 +390,12 @@ class Problem:
         out = np.empty(shape, dtype=dtype)
         _check(lib().vt_problem_get_array(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p),
                                           out.nbytes))
+        return out
+
+    def exact_state(self, t: float) -> np.ndarray:
+        """The exactly translated vortex at time t at the nodes (periodic image)."""
+        out = np.empty((self.K, self.Np, 4))
+        _check(lib().vt_problem_exact_state(self._h, float(t), _ptr(out)))
         return out
 
     def mesh_desc(self) -> vt_mesh_desc:
@@ -489,6 +519,23 @@ class Solver:
     def rhs(self) -> np.ndarray:
         out = np.empty((self.K, self.Np, 4))
         self._step_status(lib().vt_rhs(self._h, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def save(self, path: str) -> None:
+        """Full-precision dump of the state and time (restart with load)."""
+        _check(lib().vt_save_state(self._h, os.fsencode(path)))
+
+    def load(self, path: str) -> None:
+        _check(lib().vt_load_state(self._h, os.fsencode(path)))
+
+    def l2_error(self, U_ref, area_quad) -> np.ndarray:
+        """The reference script's L2 difference between the state and U_ref
+        (numpy, or a CUDA torch tensor on this device) with the area rule
+        area_quad (nq x 3), computed on the device."""
+        aq = np.ascontiguousarray(area_quad, dtype=np.float64).reshape(-1, 3)
+        ins, _outp, _out, dev, _keep = self._state_args(U_ref)
+        out = np.empty(4)
+        _check(lib().vt_l2_error(self._h, aq.shape[0], _ptr(aq), ins[0], dev, _ptr(out)))
         return out
 
     def totals(self) -> np.ndarray:

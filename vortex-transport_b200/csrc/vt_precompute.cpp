@@ -567,6 +567,25 @@ void reference_to_physical(const double* vtx, double xi, double eta, double* x, 
 
 }  // namespace
 
+void exact_vortex(const vt_params& prm, const vt_vortex& ic, const std::vector<double>& nodes_phys, double t,
+                  double* U) {
+  const double Lx = prm.domain_x, Ly = prm.domain_y;
+  const size_t n = nodes_phys.size() / 2;
+  for (size_t a = 0; a < n; ++a) {
+    double x = nodes_phys[2 * a], y = nodes_phys[2 * a + 1];
+    // shift the node by whole periods so it lies within half a period of the centre
+    x -= Lx * std::nearbyint((x - ic.x0 - ic.U_infty * t) / Lx);
+    y -= Ly * std::nearbyint((y - ic.y0 - ic.V_infty * t) / Ly);
+    double rho, u, v, pr;
+    vortex_state(ic, x, y, t, &rho, &u, &v, &pr);
+    const double E = pr / (rho * (ic.gamma - 1.0)) + (std::pow(u, 2.0) + std::pow(v, 2.0)) / 2.0;
+    U[4 * a + 0] = rho;
+    U[4 * a + 1] = rho * u;
+    U[4 * a + 2] = rho * v;
+    U[4 * a + 3] = rho * E;
+  }
+}
+
 void flux_from_state(int K, int Np, const double* U, double* F) {
   const double gamma = 1.4;
   for (size_t a = 0; a < static_cast<size_t>(K) * Np; ++a) {

@@ -73,6 +73,13 @@ int initial_condition(const vt_params& prm, const vt_vortex& ic, const Mesh& mes
                       const std::vector<double>& minv_ref, double time, std::vector<double>* U,
                       std::vector<double>* F, std::vector<double>* nodes_phys);
 
+// The exactly translated vortex at time t at the physical nodes (K x Np x 2),
+// U = K x Np x 4: the formula of Element.cpp:134-179 with the centre moved by
+// (U_infty, V_infty) t and taken as the nearest periodic image of each node on
+// the domain_x x domain_y torus (the reference's formula does not wrap).
+void exact_vortex(const vt_params& prm, const vt_vortex& ic, const std::vector<double>& nodes_phys, double t,
+                  double* U);
+
 // Nodal flux of a state (Timestepping.cpp:141-158 formula), F = K x Np x 2 x 4.
 void flux_from_state(int K, int Np, const double* U, double* F);
 

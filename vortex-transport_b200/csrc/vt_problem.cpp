@@ -203,4 +203,71 @@ int vt_flux_from_state(int K, int p, const double* U, double* F) {
   return VT_OK;
 }
 
+int vt_problem_exact_state(const vt_problem* pb, double t, double* U) {
+  if (!pb || !U) return vt::fail(VT_ERR_INVALID, "vt_problem_exact_state: null argument");
+  vt::exact_vortex(pb->prm, pb->ic, pb->nodes_phys, t, U);
+  return VT_OK;
+}
+
+// State file: "VTSTATE" + NUL, int32 version (1), p, K, Np, float64 time, then
+// K x Np x 4 float64 (the reference's element-major U layout), little-endian
+// as the host writes it.
+namespace {
+constexpr char kStateMagic[8] = {'V', 'T', 'S', 'T', 'A', 'T', 'E', '\0'};
+struct StateHeader {
+  char magic[8];
+  int32_t version, p, K, Np;
+  double time;
+};
+static_assert(sizeof(StateHeader) == 32, "state header layout");
+}  // namespace
+
+int vt_write_state_file(const char* path, int p, int K, double time, const double* U) {
+  if (!path || !U || p < 0 || p > 3 || K < 1) return vt::fail(VT_ERR_INVALID, "vt_write_state_file: bad argument");
+  StateHeader h{};
+  std::memcpy(h.magic, kStateMagic, 8);
+  h.version = 1;
+  h.p = p;
+  h.K = K;
+  h.Np = vt::np_of(p);
+  h.time = time;
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) return vt::fail(VT_ERR_INVALID, std::string("vt_write_state_file: cannot open '") + path + "'");
+  f.write(reinterpret_cast<const char*>(&h), sizeof(h));
+  f.write(reinterpret_cast<const char*>(U), static_cast<std::streamsize>(sizeof(double) * 4 * static_cast<size_t>(K) * h.Np));
+  if (!f) return vt::fail(VT_ERR_INVALID, std::string("vt_write_state_file: write failed on '") + path + "'");
+  return VT_OK;
+}
+
+int vt_state_file_info(const char* path, int* p, int* K, double* time) {
+  if (!path) return vt::fail(VT_ERR_INVALID, "vt_state_file_info: null path");
+  std::ifstream f(path, std::ios::binary);
+  StateHeader h{};
+  if (!f || !f.read(reinterpret_cast<char*>(&h), sizeof(h)))
+    return vt::fail(VT_ERR_INVALID, std::string("vt_state_file_info: cannot read '") + path + "'");
+  if (std::memcmp(h.magic, kStateMagic, 8) != 0 || h.version != 1 || h.p < 0 || h.p > 3 || h.K < 1 ||
+      h.Np != vt::np_of(h.p))
+    return vt::fail(VT_ERR_INVALID, std::string("vt_state_file_info: '") + path + "' is not a state file");
+  f.seekg(0, std::ios::end);
+  const std::streamoff want = static_cast<std::streamoff>(sizeof(h) + sizeof(double) * 4 * static_cast<size_t>(h.K) * h.Np);
+  if (f.tellg() != want) return vt::fail(VT_ERR_INVALID, std::string("vt_state_file_info: '") + path + "' has the wrong size");
+  if (p) *p = h.p;
+  if (K) *K = h.K;
+  if (time) *time = h.time;
+  return VT_OK;
+}
+
+int vt_read_state_file(const char* path, double* U) {
+  int p = 0, K = 0;
+  double t = 0;
+  int st = vt_state_file_info(path, &p, &K, &t);
+  if (st) return st;
+  if (!U) return vt::fail(VT_ERR_INVALID, "vt_read_state_file: null output");
+  std::ifstream f(path, std::ios::binary);
+  f.seekg(sizeof(StateHeader));
+  if (!f.read(reinterpret_cast<char*>(U), static_cast<std::streamsize>(sizeof(double) * 4 * static_cast<size_t>(K) * vt::np_of(p))))
+    return vt::fail(VT_ERR_INVALID, std::string("vt_read_state_file: cannot read '") + path + "'");
+  return VT_OK;
+}
+
 }  // extern "C"

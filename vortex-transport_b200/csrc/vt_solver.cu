@@ -114,6 +114,46 @@ __global__ void totals_partial_kernel(const double2* __restrict__ U, const doubl
   if (threadIdx.x < 4) partial[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
+// The L2 difference of two states in the form of the reference's
+// post-processing script (plottools/l2stateerror.py:65-98): per element the
+// squared nodal differences, interpolated at the area-rule points (bq: nq x Np
+// basis values), integrated with the rule weights and det J. Per-block partial
+// sums in a fixed order, summed by totals_final_kernel.
+__global__ void l2_partial_kernel(const double2* __restrict__ U, const double2* __restrict__ V,
+                                  const double2* __restrict__ geo, const double* __restrict__ bq,
+                                  const double* __restrict__ wq, int nq, int K, int Np, long long Kpad,
+                                  double* __restrict__ partial) {
+  __shared__ double red[4][256];
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[4] = {0, 0, 0, 0};
+  if (e < K) {
+    double del[10][4];
+    for (int j = 0; j < Np; ++j) {
+      const double2 a = U[(2 * j) * Kpad + e], b = U[(2 * j + 1) * Kpad + e];
+      const double2 c = V[(2 * j) * Kpad + e], d = V[(2 * j + 1) * Kpad + e];
+      const double x[4] = {a.x - c.x, a.y - c.y, b.x - d.x, b.y - d.y};
+      for (int k = 0; k < 4; ++k) del[j][k] = x[k] * x[k];
+    }
+    for (int k = 0; k < 4; ++k) {
+      double s = 0.0;
+      for (int q = 0; q < nq; ++q) {
+        double v = 0.0;
+        for (int j = 0; j < Np; ++j) v += del[j][k] * bq[q * Np + j];
+        s += wq[q] * v;
+      }
+      acc[k] = geo[6 * Kpad + e].y * s;
+    }
+  }
+  for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) partial[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
 __global__ void totals_final_kernel(const double* __restrict__ partial, int nblocks,
                                     double* __restrict__ out) {
   __shared__ double red[4][256];
@@ -565,6 +605,68 @@ int vt_totals(vt_ctx* c, double* out) {
   if (!e) e = cudaMemcpyAsync(out, c->tot, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (!e) e = cudaStreamSynchronize(c->stream);
   return e ? fail(VT_ERR_CUDA, vt::cuda_msg("totals", e)) : VT_OK;
+}
+
+int vt_l2_error(vt_ctx* c, int nq, const double* area_quad, const double* U_ref, int device_pointers, double* out) {
+  if (!c || nq < 1 || !area_quad || !U_ref || !out) return fail(VT_ERR_INVALID, "vt_l2_error: bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const int Np = c->Np;
+  std::vector<double> tab(static_cast<size_t>(nq) * (Np + 1));
+  for (int q = 0; q < nq; ++q) {
+    vt::basis(c->p, area_quad[3 * q], area_quad[3 * q + 1], &tab[static_cast<size_t>(q) * Np]);
+    tab[static_cast<size_t>(nq) * Np + q] = area_quad[3 * q + 2];
+  }
+  double* dtab = nullptr;
+  cudaError_t e = alloc(&dtab, sizeof(double) * tab.size());
+  if (!e) e = cudaMemcpyAsync(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->stream);
+  if (!e && !device_pointers) {
+    const int st = ensure_aos(c);
+    if (st) {
+      cudaFree(dtab);
+      return st;
+    }
+    e = cudaMemcpyAsync(c->aos, U_ref, sizeof(double) * 4 * static_cast<size_t>(c->K) * Np, cudaMemcpyHostToDevice,
+                        c->stream);
+  }
+  if (!e) e = aos_to_soa(c, device_pointers ? U_ref : reinterpret_cast<const double*>(c->aos), c->Sa);
+  const int blocks = (c->K + 255) / 256;
+  if (!e) {
+    vt::l2_partial_kernel<<<blocks, 256, 0, c->stream>>>(c->U, c->Sa, c->geo, dtab, dtab + static_cast<size_t>(nq) * Np,
+                                                          nq, c->K, Np, c->Kpad, c->partial);
+    vt::totals_final_kernel<<<1, 256, 0, c->stream>>>(c->partial, blocks, c->tot);
+    e = cudaGetLastError();
+  }
+  double tot[4] = {0, 0, 0, 0};
+  if (!e) e = cudaMemcpyAsync(tot, c->tot, sizeof(tot), cudaMemcpyDeviceToHost, c->stream);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (dtab) cudaFree(dtab);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("l2 error", e));
+  for (int k = 0; k < 4; ++k) out[k] = std::sqrt((1.0 / 25.0) * tot[k]);
+  return VT_OK;
+}
+
+int vt_save_state(vt_ctx* c, const char* path) {
+  if (!c || !path) return fail(VT_ERR_INVALID, "vt_save_state: null argument");
+  std::vector<double> U(4 * static_cast<size_t>(c->K) * c->Np);
+  const int st = vt_download_state(c, U.data(), nullptr);
+  return st ? st : vt_write_state_file(path, c->p, c->K, c->time, U.data());
+}
+
+int vt_load_state(vt_ctx* c, const char* path) {
+  if (!c || !path) return fail(VT_ERR_INVALID, "vt_load_state: null argument");
+  int p = 0, K = 0;
+  double t = 0.0;
+  int st = vt_state_file_info(path, &p, &K, &t);
+  if (st) return st;
+  if (p != c->p || K != c->K)
+    return fail(VT_ERR_INVALID, "vt_load_state: the file holds p=" + std::to_string(p) + ", K=" + std::to_string(K) +
+                                    ", the context p=" + std::to_string(c->p) + ", K=" + std::to_string(c->K));
+  std::vector<double> U(4 * static_cast<size_t>(K) * c->Np);
+  if ((st = vt_read_state_file(path, U.data()))) return st;
+  if ((st = vt_upload_state(c, U.data()))) return st;
+  c->time = t;
+  return VT_OK;
 }
 
 void* vt_stream(vt_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
