@@ -195,6 +195,13 @@ int vt_totals(vt_ctx* ctx, double* out);
 int vt_l2_error(vt_ctx* ctx, int nq, const double* area_quad, const double* U_ref, int device_pointers,
                 double* out);
 
+/* Sets the state to the L2 projection of the vortex `ic` at time t on the
+ * device (U_initialization_type=1, Element.cpp:180-326): vertices is the
+ * problem's K x 3 x 2 host array (vt_problem_get_array "vertices"), area_quad
+ * the nq x 3 area rule (xi, eta, weight). */
+int vt_project_vortex(vt_ctx* ctx, const double* vertices, const vt_vortex* ic, double t, int nq,
+                      const double* area_quad);
+
 /* Full-precision dump and restart, replacing the reference's 6-decimal
  * per-element text dumps (Element::write_data, Element.cpp:336-425) where a
  * run must resume exactly. A state file is "VTSTATE" + NUL, int32 version (1),

@@ -168,6 +168,8 @@ _SIGNATURES = {
     "vt_batch_set_blocks_per_sm": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "vt_checkpoint_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "vt_save_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "vt_project_vortex": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(vt_vortex), ctypes.c_double,
+                                         ctypes.c_int, _dp]),
     "vt_load_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "vt_write_state_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
     "vt_state_file_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
@@ -520,6 +522,14 @@ class Solver:
         out = np.empty((self.K, self.Np, 4))
         self._step_status(lib().vt_rhs(self._h, out.ctypes.data_as(ctypes.c_void_p)))
         return out
+
+    def project_vortex(self, problem: "Problem", ic: vt_vortex | None = None, t: float = 0.0) -> None:
+        """State = L2 projection of the vortex (default: the reference's) onto
+        the basis, computed on the device with the problem's area rule."""
+        verts = np.ascontiguousarray(problem.array("vertices"))
+        aq = np.ascontiguousarray(problem.array("area_quad"))
+        ic = ic if ic is not None else default_vortex()
+        _check(lib().vt_project_vortex(self._h, _ptr(verts), ctypes.byref(ic), float(t), aq.shape[0], _ptr(aq)))
 
     def save(self, path: str) -> None:
         """Full-precision dump of the state and time (restart with load)."""

@@ -32,6 +32,7 @@ struct vt_ctx {
   double2* aos = nullptr;
   double *W = nullptr, *partial = nullptr, *tot = nullptr;
   std::vector<double> ops;
+  std::vector<double> minv_ref;  // Np x Np, for the projected initial condition
   vt::LaunchFn launch = nullptr;
   double time = 0.0;
   cudaGraphExec_t rk4_graph = nullptr;

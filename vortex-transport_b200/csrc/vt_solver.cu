@@ -154,6 +154,61 @@ __global__ void l2_partial_kernel(const double2* __restrict__ U, const double2* 
   if (threadIdx.x < 4) partial[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
+// The isentropic vortex (Element.cpp:134-179 formula, parameters from `ic`).
+__device__ void vortex_point(const vt_vortex& c, double x, double y, double t, double* s) {
+  const double dx = x - c.x0 - c.U_infty * t, dy = y - c.y0 - c.V_infty * t;
+  const double f0 = 1.0 - (dx * dx + dy * dy) / (c.rc * c.rc);
+  const double f1 = 1.0 - c.epsilon * c.epsilon * (c.gamma - 1) * (c.M_infty * c.M_infty) * exp(f0) /
+                              (8.0 * (M_PI * M_PI));
+  const double f2 = c.epsilon * (c.U_infty * c.U_infty + c.V_infty * c.V_infty) * exp(f0 / 2.0) / (2.0 * M_PI * c.rc);
+  const double rho = c.rho_infty * pow(f1, 1.0 / (c.gamma - 1.0));
+  const double u = c.U_infty - f2 * dy, v = c.V_infty + f2 * dx;
+  const double p = c.p_infty * pow(f1, c.gamma / (c.gamma - 1.0));
+  const double E = p / (rho * (c.gamma - 1.0)) + (u * u + v * v) / 2.0;
+  s[0] = rho;
+  s[1] = rho * u;
+  s[2] = rho * v;
+  s[3] = rho * E;
+}
+
+// L2 projection of the vortex onto each element's basis (Element.cpp:180-326):
+// b_i = sum_q detJ phi_i(q) u(x_q) w_q, U_i = sum_j (M_ref^-1_ij / detJ) b_j, with
+// x_q the affine image of the area-rule point. One thread per element; tab
+// holds the basis at the points (nq x Np), the weights (nq), the points (nq x 2)
+// and M_ref^-1 (Np x Np).
+__global__ void project_vortex_kernel(const double* __restrict__ verts, const double2* __restrict__ geo,
+                                      const double* __restrict__ tab, int nq, const vt_vortex ic, double t, int K,
+                                      int Np, long long Kpad, double2* __restrict__ U) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= K) return;
+  const double* bq = tab;
+  const double* wq = tab + nq * Np;
+  const double* pq = wq + nq;
+  const double* minv = pq + 2 * nq;
+  const double* v = verts + 6 * static_cast<long long>(e);
+  const double det = geo[6 * Kpad + e].y;
+  double b[10][4];
+  for (int i = 0; i < Np; ++i)
+    for (int k = 0; k < 4; ++k) b[i][k] = 0.0;
+  for (int q = 0; q < nq; ++q) {
+    const double xi = pq[2 * q], eta = pq[2 * q + 1];
+    const double h0 = 1.0 - xi - eta;
+    const double x = v[0] * h0 + v[2] * xi + v[4] * eta;
+    const double y = v[1] * h0 + v[3] * xi + v[5] * eta;
+    double s[4];
+    vortex_point(ic, x, y, t, s);
+    for (int i = 0; i < Np; ++i)
+      for (int k = 0; k < 4; ++k) b[i][k] += det * bq[q * Np + i] * s[k] * wq[q];
+  }
+  for (int i = 0; i < Np; ++i) {
+    double r[4] = {0, 0, 0, 0};
+    for (int j = 0; j < Np; ++j)
+      for (int k = 0; k < 4; ++k) r[k] += (minv[i * Np + j] / det) * b[j][k];
+    U[(2 * i) * Kpad + e] = make_double2(r[0], r[1]);
+    U[(2 * i + 1) * Kpad + e] = make_double2(r[2], r[3]);
+  }
+}
+
 __global__ void totals_final_kernel(const double* __restrict__ partial, int nblocks,
                                     double* __restrict__ out) {
   __shared__ double red[4][256];
@@ -355,6 +410,7 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
   c->max_blocks = sms * (per_sm > 0 ? per_sm : 1);
   c->ops = vt::fold_operators(c->p, c->nfq, d->inv_mass_ref, d->stiffness_ref, d->line_quadrature,
                               d->phi_plus, d->phi_minus);
+  c->minv_ref.assign(d->inv_mass_ref, d->inv_mass_ref + c->Np * c->Np);
 
   // packed geometry and side-ordered neighbours (Evolve.cpp:167-202)
   const long long KP = c->Kpad;
@@ -644,6 +700,37 @@ int vt_l2_error(vt_ctx* c, int nq, const double* area_quad, const double* U_ref,
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("l2 error", e));
   for (int k = 0; k < 4; ++k) out[k] = std::sqrt((1.0 / 25.0) * tot[k]);
   return VT_OK;
+}
+
+int vt_project_vortex(vt_ctx* c, const double* vertices, const vt_vortex* ic, double t, int nq,
+                      const double* area_quad) {
+  if (!c || !vertices || !ic || nq < 1 || !area_quad) return fail(VT_ERR_INVALID, "vt_project_vortex: bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const int Np = c->Np;
+  std::vector<double> tab(static_cast<size_t>(nq) * (Np + 3) + Np * Np);
+  for (int q = 0; q < nq; ++q) {
+    vt::basis(c->p, area_quad[3 * q], area_quad[3 * q + 1], &tab[static_cast<size_t>(q) * Np]);
+    tab[static_cast<size_t>(nq) * Np + q] = area_quad[3 * q + 2];
+    tab[static_cast<size_t>(nq) * (Np + 1) + 2 * q] = area_quad[3 * q];
+    tab[static_cast<size_t>(nq) * (Np + 1) + 2 * q + 1] = area_quad[3 * q + 1];
+  }
+  std::copy(c->minv_ref.begin(), c->minv_ref.end(), tab.begin() + static_cast<size_t>(nq) * (Np + 3));
+  double *dtab = nullptr, *dverts = nullptr;
+  const size_t vbytes = sizeof(double) * 6 * static_cast<size_t>(c->K);
+  cudaError_t e = alloc(&dtab, sizeof(double) * tab.size());
+  if (!e) e = alloc(&dverts, vbytes);
+  if (!e) e = cudaMemcpyAsync(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->stream);
+  if (!e) e = cudaMemcpyAsync(dverts, vertices, vbytes, cudaMemcpyHostToDevice, c->stream);
+  if (!e) {
+    vt::project_vortex_kernel<<<(c->K + 127) / 128, 128, 0, c->stream>>>(dverts, c->geo, dtab, nq, *ic, t, c->K, Np,
+                                                                        c->Kpad, c->U);
+    e = cudaGetLastError();
+  }
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (dtab) cudaFree(dtab);
+  if (dverts) cudaFree(dverts);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("project vortex", e)) : VT_OK;
 }
 
 int vt_save_state(vt_ctx* c, const char* path) {
