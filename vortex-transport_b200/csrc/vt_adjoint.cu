@@ -123,6 +123,7 @@ struct AdjointState {
   double2 *bp = nullptr, *bm = nullptr;  // face adjoints
   // edge-once face phase: owner elements (null when the mesh does not 2-colour)
   int* owners = nullptr;
+  int* owner_nb = nullptr;  // [3][nowners]
   unsigned char* is_owner = nullptr;
   int nowners = 0;
   double2* slots = nullptr;
@@ -195,9 +196,17 @@ int setup(vt_ctx* c) {
       flag[x] = col[x] == 0;
       if (flag[x]) owners.push_back(x);
     }
-    s->nowners = static_cast<int>(owners.size());
+    const size_t no = owners.size();
+    s->nowners = static_cast<int>(no);
+    // owners, then their neighbours per side, then the owner flags
+    for (int sd = 0; sd < 3; ++sd)
+      for (size_t i = 0; i < no; ++i) {
+        const int4 b = nb[owners[i]];
+        owners.push_back(sd == 0 ? b.x : (sd == 1 ? b.y : b.z));
+      }
     e = cudaMalloc(reinterpret_cast<void**>(&s->owners), sizeof(int) * owners.size() + flag.size());
     if (!e) {
+      s->owner_nb = s->owners + no;
       s->is_owner = reinterpret_cast<unsigned char*>(s->owners + owners.size());
       e = cudaMemcpy(s->owners, owners.data(), sizeof(int) * owners.size(), cudaMemcpyHostToDevice);
     }
@@ -266,6 +275,7 @@ AdjArgs adj_args(vt_ctx* c) {
   a.bp = c->adj->bp;
   a.bm = c->adj->bm;
   a.owners = c->adj->owners;
+  a.owner_nb = c->adj->owner_nb;
   a.is_owner = c->adj->is_owner;
   a.nowners = c->adj->nowners;
   a.geo = c->geo;

@@ -51,6 +51,7 @@ struct AdjArgs {
   // elements split into owners and non-owners with every edge joining one of
   // each; an owner evaluates each of its edges once for both sides.
   const int* owners;                // owner elements, nowners of them
+  const int* owner_nb;              // [3][nowners]: each owner's neighbour across side s
   const unsigned char* is_owner;    // K flags, or null
   int nowners;
   long long Kpad;
@@ -118,22 +119,19 @@ template <int P, int NFQ>
 __global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 3 : 2)
     adjoint_edge_kernel(const AdjArgs a, const StageOps<P, NFQ> o) {
   constexpr int NP = np_of_p(P), NE = P + 1;
-  constexpr int RA = 2 * NP, RU = 2 * NE, ROWS = 2 * RA + 2 * RU;
-  __shared__ double2 sh[ROWS][kAdjRun];  // a(e), a(nb), U(e) side nodes, U(nb) side nodes
+  constexpr int RA = 2 * NP, RU = 2 * NE, RG = 2 * RA + 2 * RU, ROWS = RG + 5;
+  // a(e), a(nb), U(e) side nodes, U(nb) side nodes, then geometry: rows 5-6 of
+  // e and of nb (side lengths / det J) and the normal of side s of e
+  __shared__ double2 sh[ROWS][kAdjRun];
   __shared__ int sE[kAdjRun], sN[kAdjRun];
   const int s = blockIdx.y, q = threadIdx.y;  // uniform per block / warp
   const int lane = threadIdx.x, tid = q * kAdjRun + lane;
   const int i0 = blockIdx.x * kAdjRun;
   const long long KP = a.Kpad;
   if (tid < kAdjRun) {
-    const int e = i0 + tid < a.nowners ? __ldg(a.owners + i0 + tid) : -1;
-    int nb = -1;
-    if (e >= 0) {
-      const int4 nb4 = __ldg(a.nbr + e);
-      nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
-    }
-    sE[tid] = e;
-    sN[tid] = nb;
+    const bool ok = i0 + tid < a.nowners;
+    sE[tid] = ok ? __ldg(a.owners + i0 + tid) : -1;
+    sN[tid] = ok ? __ldg(a.owner_nb + static_cast<long long>(s) * a.nowners + i0 + tid) : -1;
   }
   __syncthreads();
   for (int l = tid; l < ROWS * kAdjRun; l += kAdjRun * NFQ) {
@@ -145,15 +143,18 @@ __global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 3 : 2)
       v = __ldg(a.a + row * KP + e);
     } else if (row < 2 * RA) {
       v = __ldg(a.a + (row - RA) * KP + nb);
-    } else {
+    } else if (row < RG) {
       const int r = row < 2 * RA + RU ? row - 2 * RA : row - 2 * RA - RU;
       const int node = edge_node(P, s, r >> 1);
       v = __ldg(a.U + (2 * node + (r & 1)) * KP + (row < 2 * RA + RU ? e : nb));
+    } else {
+      const int g = row - RG;  // 0,1: rows 5,6 of e; 2,3: rows 5,6 of nb; 4: normal of side s
+      v = g < 4 ? __ldg(a.geo + (5 + (g & 1)) * KP + (g < 2 ? e : nb)) : __ldg(a.geo + (2 + s) * KP + e);
     }
     sh[row][ln] = v;
   }
   __syncthreads();
-  const int e = sE[lane], nb = sN[lane];
+  const int e = sE[lane];
   if (e < 0) return;
   const int qm = NFQ - 1 - q, w = s * NFQ + q;
   double up[4] = {0.0, 0.0, 0.0, 0.0}, um[4] = {0.0, 0.0, 0.0, 0.0};
@@ -187,14 +188,14 @@ __global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 3 : 2)
     bn[2] = fma(lm, c1.x, bn[2]);
     bn[3] = fma(lm, c1.y, bn[3]);
   }
-  const double2 lea = __ldg(a.geo + 5 * KP + e), leb = __ldg(a.geo + 6 * KP + e);
-  const double2 lna = __ldg(a.geo + 5 * KP + nb), lnb = __ldg(a.geo + 6 * KP + nb);
+  const double2 lea = sh[RG][lane], leb = sh[RG + 1][lane];
+  const double2 lna = sh[RG + 2][lane], lnb = sh[RG + 3][lane];
   const double se = -(s == 0 ? lea.x : (s == 1 ? lea.y : leb.x)) * a.sa;
   const double sn = (s == 0 ? lna.x : (s == 1 ? lna.y : lnb.x)) * a.sa;
   double bf[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) bf[c] = fma(se, be[c], sn * bn[c]);
-  const double2 n = __ldg(a.geo + (2 + s) * KP + e);
+  const double2 n = sh[RG + 4][lane];
   double bu[4] = {0.0, 0.0, 0.0, 0.0}, bv[4] = {0.0, 0.0, 0.0, 0.0};
   roe_flux_vjp(up, um, n.x, n.y, bf, bu, bv);
   const long long r0 = static_cast<long long>(2 * w) * KP + e;
@@ -212,9 +213,27 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P))
   const int e = blockIdx.x * kAdjRun + threadIdx.x;
   const int j = threadIdx.y;  // node, uniform per warp
   const long long KP = a.Kpad;
+  // every global operand of this thread is requested before the barrier
+  const long long r0 = (2 * j) * KP + e, r1 = r0 + KP;
+  double2 u0 = make_double2(1.0, 0.0), u1 = make_double2(0.0, 0.0), j0 = u1, j1 = u1, l0 = u1, l1 = u1, c0 = u1,
+          c1 = u1;
+  int4 nb4 = make_int4(0, 0, 0, 0);
   if (e < a.K) {
     sA[2 * j][threadIdx.x] = __ldg(a.a + (2 * j) * KP + e);
     sA[2 * j + 1][threadIdx.x] = __ldg(a.a + (2 * j + 1) * KP + e);
+    u0 = __ldg(a.U + r0);
+    u1 = __ldg(a.U + r1);
+    j0 = __ldg(a.geo + 0 * KP + e);
+    j1 = __ldg(a.geo + 1 * KP + e);
+    nb4 = __ldg(a.nbr + e);
+    if (a.lam_coef != 0.0 || a.a_out) {
+      l0 = a.lam[r0];
+      l1 = a.lam[r1];
+    }
+    if (a.acc_in) {
+      c0 = a.acc_in[r0];
+      c1 = a.acc_in[r1];
+    }
   }
   __syncthreads();
   if (e >= a.K) return;
@@ -239,12 +258,9 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P))
       bx[c] *= a.sa;
       by[c] *= a.sa;
     }
-    const double2 j0 = __ldg(a.geo + 0 * KP + e), j1 = __ldg(a.geo + 1 * KP + e);
-    const double2 u0 = __ldg(a.U + (2 * j) * KP + e), u1 = __ldg(a.U + (2 * j + 1) * KP + e);
     const double sv[4] = {u0.x, u0.y, u1.x, u1.y};
     contravariant_vjp(sv, j0.x, j0.y, j1.x, j1.y, bx, by, g);
   }
-  const int4 nb4 = __ldg(a.nbr + e);
   // two-sided faces: own bp (tp) and the neighbour's bm (tm); edge-once: an
   // owner takes bp of its evaluation, a non-owner bm of its neighbour's
   const bool use_p = !a.is_owner || a.is_owner[e];
@@ -277,23 +293,8 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P))
       }
     }
   }
-  const long long r0 = (2 * j) * KP + e, r1 = r0 + KP;
-  double lam[4] = {0.0, 0.0, 0.0, 0.0};
-  if (a.lam_coef != 0.0 || a.a_out) {
-    const double2 l0 = a.lam[r0], l1 = a.lam[r1];
-    lam[0] = l0.x;
-    lam[1] = l0.y;
-    lam[2] = l1.x;
-    lam[3] = l1.y;
-  }
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  if (a.acc_in) {
-    const double2 c0 = a.acc_in[r0], c1 = a.acc_in[r1];
-    acc[0] = c0.x;
-    acc[1] = c0.y;
-    acc[2] = c1.x;
-    acc[3] = c1.y;
-  }
+  const double lam[4] = {l0.x, l0.y, l1.x, l1.y};
+  double acc[4] = {c0.x, c0.y, c1.x, c1.y};
 #pragma unroll
   for (int c = 0; c < 4; ++c) acc[c] = fma(a.lam_coef, lam[c], acc[c]) + g[c];
   if (a.a_out) {
