@@ -328,6 +328,17 @@ def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0):
     return out
 
 
+def max_over_ranks(x: float, pg=None, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank's replica must be done, so the job
+    time is the maximum (all ranks call this, in the same order)."""
+    if not pg:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -395,13 +406,6 @@ def b200_arm(args):
         if pg:
             pg.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if not pg:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
-
     # warm-up (also captures the step graph)
     solver.rk4(DT, max(args.warmup, 1))
 
@@ -415,7 +419,7 @@ def b200_arm(args):
         ev1.record(stream)
         solver.synchronize()
         torch.cuda.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms = max_over_ranks(ev0.elapsed_time(ev1), pg)
     barrier()
     value = world * dof_stages_per_step * args.steps / (ms * 1e-3)
 
@@ -436,7 +440,7 @@ def b200_arm(args):
         solver.download(out=host_U)  # device -> pinned host
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg)
     e2e_value = world * dof_stages_per_step * e2e_steps / (e2e_ms * 1e-3) if e2e_steps else None
     state_bytes = K_el * NP * 4 * 8
 
