@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kAdjRun * NFQ)
 // operands every face point of an edge shares (both elements' adjoints, the
 // side's node states of both) are staged once per block in shared memory.
 template <int P, int NFQ>
-__global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 3 : 2)
+__global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 4 : 2)
     adjoint_edge_kernel(const AdjArgs a, const StageOps<P, NFQ> o) {
   constexpr int NP = np_of_p(P), NE = P + 1;
   constexpr int RA = 2 * NP, RU = 2 * NE, RG = 2 * RA + 2 * RU, ROWS = RG + 5;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 3 : 2)
 }
 
 template <int P, int NFQ>
-__global__ void __launch_bounds__(kAdjRun * np_of_p(P))
+__global__ void __launch_bounds__(kAdjRun * np_of_p(P), 3)
     adjoint_element_kernel(const AdjArgs a, const StageOps<P, NFQ> o) {
   constexpr int NP = np_of_p(P), NE = P + 1;
   __shared__ double2 sA[2 * NP][kAdjRun];  // the block's stage adjoints, row pair j loaded by warp j
