@@ -113,8 +113,21 @@ AdjKernels select_adjoint(int p, int nfq) {
 
 }  // namespace
 
+// A sweep's launches depend only on its buffers, step count and time step, so
+// a repeated sweep replays a captured CUDA graph instead of relaunching.
+struct SweepGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<long long> key;
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+  }
+};
+
 struct AdjointState {
   AdjKernels k;
+  SweepGraph fwd_graph, bwd_graph;
   size_t state_elems = 0;  // double2 entries of one state vector
   // work, stage states, adjoint, accumulator, two stage adjoints (contiguous)
   double2* bufs = nullptr;
@@ -351,6 +364,36 @@ cudaError_t lincomb(vt_ctx* c, double2* out, const double2* x, double cx, const 
   return cudaGetLastError();
 }
 
+template <typename F>
+cudaError_t run_captured(vt_ctx* c, SweepGraph& g, const std::vector<long long>& key, F&& enqueue) {
+  if (!g.exec || g.key != key) {
+    g.reset();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e) return e;
+    const cudaError_t le = enqueue();
+    e = cudaStreamEndCapture(c->stream, &graph);
+    if (le) e = le;
+    if (!e) e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e) {
+      g.reset();
+      return e;
+    }
+    g.key = key;
+  }
+  return cudaGraphLaunch(g.exec, c->stream);
+}
+
+std::vector<long long> sweep_key(vt_ctx* c, int kind) {
+  const AdjointState* s = c->adj;
+  long long dt_bits = 0;
+  std::memcpy(&dt_bits, &s->dt, sizeof(dt_bits));
+  return {kind, s->nsteps, dt_bits, s->all_stages, reinterpret_cast<long long>(s->slots), s->nslots,
+          reinterpret_cast<long long>(c->U), reinterpret_cast<long long>(s->bufs),
+          static_cast<long long>(s->first_adjoint), static_cast<long long>(s->plan.size())};
+}
+
 int prepare(vt_ctx* c) {
   int st = setup(c);
   if (!st) st = ensure_aos(c);
@@ -361,6 +404,8 @@ int prepare(vt_ctx* c) {
 
 void adjoint_release(vt_ctx* c) {
   if (!c || !c->adj) return;
+  c->adj->fwd_graph.reset();
+  c->adj->bwd_graph.reset();
   if (c->adj->owners) cudaFree(c->adj->owners);
   if (c->adj->slots) cudaFree(c->adj->slots);
   if (c->adj->bufs) cudaFree(c->adj->bufs);
@@ -394,12 +439,16 @@ int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
     s->info.stage_steps = s->info.adjoint_steps = nsteps;
     s->info.slots_used = 4 * nsteps;
     s->info.all_stages = 1;
-    cudaError_t e = cudaMemcpyAsync(vt::slot(c, 0), c->U, sizeof(double2) * s->state_elems,
-                                    cudaMemcpyDeviceToDevice, c->stream);
-    if (!e) e = vt::reset_error_words(c);
-    for (int i = 0; i < nsteps && !e; ++i)
-      e = vt::stage_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
-                         vt::slot(c, 4ll * i + 3), dt, i + 1 < nsteps ? vt::slot(c, 4ll * i + 4) : c->U);
+    cudaError_t e = vt::reset_error_words(c);
+    if (!e)
+      e = vt::run_captured(c, s->fwd_graph, vt::sweep_key(c, 0), [&]() {
+        cudaError_t x = cudaMemcpyAsync(vt::slot(c, 0), c->U, sizeof(double2) * s->state_elems,
+                                        cudaMemcpyDeviceToDevice, c->stream);
+        for (int i = 0; i < nsteps && !x; ++i)
+          x = vt::stage_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
+                             vt::slot(c, 4ll * i + 3), dt, i + 1 < nsteps ? vt::slot(c, 4ll * i + 4) : c->U);
+        return x;
+      });
     if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint forward", e));
     st = vt::finish(c, nsteps, dt);
     if (st == VT_OK) s->have_forward = s->fresh = true;
@@ -414,10 +463,13 @@ int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
     if (a.op == vt::CkptOp::kAdvance && a.dst != vt::kWorkSlot) used = std::max(used, a.dst + 1);
   if ((st = vt::ensure_slots(c, used))) return st;
   if ((st = vt_checkpoint_plan(nsteps, S, &s->info))) return st;
-  cudaError_t e = cudaMemcpyAsync(vt::slot(c, 0), c->U, sizeof(double2) * s->state_elems, cudaMemcpyDeviceToDevice,
-                                  c->stream);
-  if (!e) e = vt::reset_error_words(c);
-  if (!e) e = vt::run_plan(c, 0, s->first_adjoint, c->U);
+  cudaError_t e = vt::reset_error_words(c);
+  if (!e)
+    e = vt::run_captured(c, s->fwd_graph, vt::sweep_key(c, 1), [&]() {
+      cudaError_t x = cudaMemcpyAsync(vt::slot(c, 0), c->U, sizeof(double2) * s->state_elems,
+                                      cudaMemcpyDeviceToDevice, c->stream);
+      return x ? x : vt::run_plan(c, 0, s->first_adjoint, c->U);
+    });
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint forward", e));
   st = vt::finish(c, nsteps, dt);
   if (st == VT_OK) s->have_forward = s->fresh = true;
@@ -434,9 +486,14 @@ int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int dev
   cudaError_t e = vt::reset_error_words(c);
   if (s->all_stages) {  // nothing to recompute
     if (!e) e = vt::load_aos(c, dJdU_T, device_pointers, s->lam);
-    for (int i = s->nsteps - 1; i >= 0 && !e; --i)
-      e = vt::adjoint_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
-                           vt::slot(c, 4ll * i + 3), s->dt);
+    if (!e)
+      e = vt::run_captured(c, s->bwd_graph, vt::sweep_key(c, 2), [&]() {
+        cudaError_t x = cudaSuccess;
+        for (int i = s->nsteps - 1; i >= 0 && !x; --i)
+          x = vt::adjoint_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
+                               vt::slot(c, 4ll * i + 3), s->dt);
+        return x;
+      });
     if (!e) e = vt::store_aos(c, s->lam, dJdU_0, device_pointers);
     if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint backward", e));
     return vt::finish(c, 0, 0.0);
@@ -446,7 +503,9 @@ int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int dev
   if (!e && !s->fresh) e = vt::run_plan(c, 0, s->first_adjoint, nullptr);
   s->fresh = false;
   if (!e) e = vt::load_aos(c, dJdU_T, device_pointers, s->lam);
-  if (!e) e = vt::run_plan(c, s->first_adjoint, s->plan.size(), nullptr);
+  if (!e)
+    e = vt::run_captured(c, s->bwd_graph, vt::sweep_key(c, 3),
+                         [&]() { return vt::run_plan(c, s->first_adjoint, s->plan.size(), nullptr); });
   if (!e) e = vt::store_aos(c, s->lam, dJdU_0, device_pointers);
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint backward", e));
   return vt::finish(c, 0, 0.0);
