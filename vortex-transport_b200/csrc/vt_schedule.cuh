@@ -33,11 +33,12 @@ inline std::vector<int4> structured_tiles(int K, const int32_t* type, const int3
     if (type[i] != i % 2 || conn[3 * i] != right || conn[3 * i + 1] != left || conn[3 * i + 2] != vert)
       return tiles;
   }
-  if (nx % 16 || ny % 2) return tiles;
+  constexpr int cells = kTileRun / 2;  // cells per run
+  if (nx % cells || ny % 2) return tiles;
   for (int rp = 0; rp < ny / 2; ++rp)
-    for (int j = 0; j < nx / 16; ++j) {
-      const int s0 = 2 * nx * (2 * rp) + 32 * j;
-      tiles.push_back(make_int4(s0, 32, s0 + 2 * nx, 32));
+    for (int j = 0; j < nx / cells; ++j) {
+      const int s0 = 2 * nx * (2 * rp) + kTileRun * j;
+      tiles.push_back(make_int4(s0, kTileRun, s0 + 2 * nx, kTileRun));
     }
   return tiles;
 }

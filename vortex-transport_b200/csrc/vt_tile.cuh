@@ -116,6 +116,8 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 constexpr unsigned kMaxWaitTries = 1u << 22;
+// resident blocks per SM the shared-memory tile allows (about 73 KB per 64 elements at p = 3)
+constexpr int kStageBlocksPerSM = 3 * 64 / kTileElems;
 
 // Warp 0 issues the bulk copies of a tile's 2*Np state rows (two runs each)
 // into S, after lane 0 announced the byte count on the barrier.
@@ -139,7 +141,7 @@ __device__ __forceinline__ void issue_tile_copies(const StageArgs& a, const int4
 template <int P, int NFQ>
 // Three 256-thread blocks per SM (<= 80 registers per thread) keep 24 warps
 // resident alongside 3 x ~75 KB of shared memory.
-__global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const StageArgs a,
+__global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_kernel(const StageArgs a,
                                                                         const StageOps<P, NFQ> ops) {
   using L = TileLayout<P, NFQ>;
   constexpr int E = L::E;
@@ -203,20 +205,21 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
 
     // ---- prefetch: the next tile into L2 (its state copies start in phase 5), this
     // tile's RK rows into L2 and its geometry rows into L1 -----------------------
-    if (t < 64) {
-      if (has_next) {
-        const int4 rr = __ldg(a.tiles + tile + G);
-        const int which = t & 1, r = t >> 1;
+    if (has_next) {  // next tile: 2 Np state rows, 7 geometry rows and the neighbour row, two runs each
+      const int4 rr = __ldg(a.tiles + tile + G);
+      for (int l = t; l < 2 * (2 * NP + 8); l += T) {
+        const int which = l & 1, r = l >> 1;
         const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
         if (len > 0) {
           const unsigned bytes = static_cast<unsigned>(len) * 16u;
           if (r < 2 * NP) prefetch_l2(a.in + r * KP + start, bytes);
           else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
-          else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
+          else prefetch_l2(a.nbr + start, bytes);
         }
       }
-    } else if (t < 64 + 8 * NP) {
-      const int l = t - 64, which = l & 1, r = l >> 1;
+    }
+    for (int l = t; l < 2 * 4 * NP; l += T) {  // this tile's RK accumulator and base rows
+      const int which = l & 1, r = l >> 1;
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
       if (len > 0) {
         const unsigned bytes = static_cast<unsigned>(len) * 16u;
@@ -226,11 +229,14 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
           prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
         }
       }
-    } else if (t < 64 + 8 * NP + 56) {
-      // this tile's 7 geometry rows into L1 (4 lines per 32-element run)
-      const int l = t - 64 - 8 * NP, row = l >> 3, which = (l >> 2) & 1, line = l & 3;
-      const int start = which ? run.z : run.x, len = which ? run.w : run.y;
-      if (line * 8 < len) prefetch_l1(a.geo + row * KP + start + line * 8);
+    }
+    {  // this tile's 7 geometry rows into L1 (128-byte lines, kTileRun / 8 per run)
+      constexpr int LPR = kTileRun / 8;
+      for (int l = t; l < 7 * 2 * LPR; l += T) {
+        const int row = l / (2 * LPR), which = (l / LPR) & 1, line = l % LPR;
+        const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+        if (line * 8 < len) prefetch_l1(a.geo + row * KP + start + line * 8);
+      }
     }
 
     // ---- 1. load ------------------------------------------------------------------
