@@ -150,6 +150,15 @@ typedef struct vt_error_info {
  * the per-step work of rk4 / forward_euler (Timestepping.H:8-9). */
 vt_ctx* vt_create(const vt_mesh_desc* desc, int device, int* status);
 void vt_destroy(vt_ctx* ctx);
+/* The whole set-up on the device for the reference's own mesh: the periodic
+ * structured triangulation with its perturbation (Meshgeneration.cpp:16-186),
+ * the per-element geometry (Element.cpp:54-93) and the initial condition
+ * (nodal or projected, Element.cpp:119-333, vortex `ic` or the reference's when
+ * NULL) are generated per element on the GPU; only the reference-space tables
+ * are built on the host. The mesh perturbation uses CUDA's sin/cos/pow, so
+ * perturbed vertices agree with vt_problem_create's (glibc) to rounding; the
+ * connectivity is identical. */
+vt_ctx* vt_create_structured(const vt_params* prm, const vt_vortex* ic, int device, int* status);
 
 /* State transfer with host arrays in the reference layout (U: K x Np x 4). */
 int vt_upload_state(vt_ctx* ctx, const double* U);

@@ -134,6 +134,8 @@ _SIGNATURES = {
     "vt_create": (ctypes.c_void_p, [ctypes.POINTER(vt_mesh_desc), ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_int)]),
     "vt_destroy": (None, [ctypes.c_void_p]),
+    "vt_create_structured": (ctypes.c_void_p, [ctypes.POINTER(vt_params), ctypes.POINTER(vt_vortex), ctypes.c_int,
+                                               ctypes.POINTER(ctypes.c_int)]),
     "vt_upload_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "vt_download_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "vt_upload_state_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -475,6 +477,24 @@ class Solver:
         self.device = device
         if U0 is not None:
             self.upload(U0)
+
+    @classmethod
+    def structured(cls, params: vt_params, ic: vt_vortex | None = None, device: int = 0) -> "Solver":
+        """A solver whose mesh, geometry and initial state are generated on the
+        device (vt_create_structured): no host precompute of per-element data."""
+        self = cls.__new__(cls)
+        self._keep = None
+        st = ctypes.c_int(0)
+        self._h = lib().vt_create_structured(ctypes.byref(params), ctypes.byref(ic) if ic is not None else None,
+                                             device, ctypes.byref(st))
+        if not self._h:
+            raise VortexError(st.value, _message())
+        self.p = params.p
+        self.Np = (params.p + 1) * (params.p + 2) // 2
+        self.K = 2 * params.num_element_in_x * params.num_element_in_y
+        self.nfq = None
+        self.device = device
+        return self
 
     # state transfer ---------------------------------------------------------
     def upload(self, U: np.ndarray) -> None:

@@ -75,6 +75,8 @@ std::vector<int4> structured_tile_runs(int K, const int32_t* type, const int32_t
   return structured_tiles(K, type, conn);
 }
 
+std::vector<int4> grid_tile_runs(int nx, int ny) { return grid_tiles(nx, ny); }
+
 cudaError_t launch_contiguous_tiles(int4* tiles, int K, int ntiles, cudaStream_t st) {
   contiguous_tiles_kernel<<<(ntiles + 255) / 256, 256, 0, st>>>(tiles, K, ntiles);
   return cudaGetLastError();

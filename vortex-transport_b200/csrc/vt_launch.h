@@ -29,6 +29,8 @@ int stage_ops_doubles(int p, int nfq);
 
 // Two-row tiles for the reference's structured mesh, empty if `conn` is not it.
 std::vector<int4> structured_tile_runs(int K, const int32_t* type, const int32_t* conn);
+// The same runs from the grid size alone (empty unless nx, ny suit them).
+std::vector<int4> grid_tile_runs(int nx, int ny);
 
 // Device-side: tiles of 64 consecutive elements, then the per-tile face lists.
 cudaError_t launch_contiguous_tiles(int4* tiles, int K, int ntiles, cudaStream_t st);

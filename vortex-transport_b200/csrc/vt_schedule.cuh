@@ -14,8 +14,22 @@
 
 namespace vt {
 
-// Two-row tiles when `conn`/`type` are exactly the reference's periodic
-// structured mesh with nx a multiple of 16 and ny even; empty otherwise.
+// Two-row tiles of the reference's structured mesh with nx x ny cells (nx a
+// multiple of kTileRun / 2 and ny even); empty otherwise.
+inline std::vector<int4> grid_tiles(int nx, int ny) {
+  std::vector<int4> tiles;
+  constexpr int cells = kTileRun / 2;  // cells per run
+  if (nx < 1 || ny < 1 || nx % cells || ny % 2) return tiles;
+  for (int rp = 0; rp < ny / 2; ++rp)
+    for (int j = 0; j < nx / cells; ++j) {
+      const int s0 = 2 * nx * (2 * rp) + kTileRun * j;
+      tiles.push_back(make_int4(s0, kTileRun, s0 + 2 * nx, kTileRun));
+    }
+  return tiles;
+}
+
+// grid_tiles when `conn`/`type` are exactly the reference's periodic
+// structured mesh; empty otherwise.
 inline std::vector<int4> structured_tiles(int K, const int32_t* type, const int32_t* conn) {
   std::vector<int4> tiles;
   if (K < 2 || conn[1] < 1) return tiles;
@@ -33,14 +47,7 @@ inline std::vector<int4> structured_tiles(int K, const int32_t* type, const int3
     if (type[i] != i % 2 || conn[3 * i] != right || conn[3 * i + 1] != left || conn[3 * i + 2] != vert)
       return tiles;
   }
-  constexpr int cells = kTileRun / 2;  // cells per run
-  if (nx % cells || ny % 2) return tiles;
-  for (int rp = 0; rp < ny / 2; ++rp)
-    for (int j = 0; j < nx / cells; ++j) {
-      const int s0 = 2 * nx * (2 * rp) + kTileRun * j;
-      tiles.push_back(make_int4(s0, kTileRun, s0 + 2 * nx, kTileRun));
-    }
-  return tiles;
+  return grid_tiles(nx, ny);
 }
 
 __global__ void contiguous_tiles_kernel(int4* tiles, int K, int ntiles) {

@@ -209,6 +209,82 @@ __global__ void project_vortex_kernel(const double* __restrict__ verts, const do
   }
 }
 
+// ---- the reference's structured periodic mesh, generated on the device --------
+// Meshgeneration.cpp:16-186 and Element.cpp:54-93 per element, with the
+// parameter block's float arithmetic kept where the reference has it (the
+// grid spacing and origin are float expressions widened to double). sin, cos
+// and pow are CUDA's, so perturbed vertices agree with the host's (glibc) to
+// rounding; connectivity is exact.
+struct GridSpec {
+  int nx, ny;
+  double gx0, gy0, esx, esy;  // origin and spacing, as the reference rounds them
+  float pg;                    // perturb_grid
+  double nodes_ref[20];        // Np x 2 reference nodes
+};
+
+__device__ void grid_point(const GridSpec& g, int a, int b, double* x, double* y) {
+  // products and sums rounded one at a time, as the host build (no contraction) does
+  const double gx = __dadd_rn(g.gx0, __dmul_rn(g.esx, b)), gy = __dadd_rn(g.gy0, __dmul_rn(g.esy, a));
+  const int inner = (a == 0 ? 0 : 1) * (a == g.ny ? 0 : 1) * (b == 0 ? 0 : 1) * (b == g.nx ? 0 : 1);
+  const float ip = static_cast<float>(inner) * g.pg;
+  const double cx = __dmul_rn(__dmul_rn(static_cast<double>(ip), 0.2), g.esx);
+  const double cy = __dmul_rn(__dmul_rn(static_cast<double>(ip), 0.2), g.esy);
+  *x = __dadd_rn(gx, __dmul_rn(cx, sin(pow(gx + 6, gy + 6))));
+  *y = __dadd_rn(gy, __dmul_rn(cy, cos(pow(gy + 6, gx + 6))));
+}
+
+// One thread per element: vertices, packed geometry rows, side-ordered
+// neighbours, and (when U is given) the nodal vortex state at the nodes.
+__global__ void structured_mesh_kernel(const GridSpec g, int Np, long long Kpad, double* __restrict__ verts,
+                                       double2* __restrict__ geo, int4* __restrict__ nbr, const vt_vortex ic,
+                                       double2* __restrict__ U) {
+  const int K = 2 * g.nx * g.ny;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= K) return;
+  const int nx = g.nx, ny = g.ny;
+  const int cell = e >> 1, r = cell / nx, j = cell % nx;
+  const bool even = (e & 1) == 0;
+  // vertex grid points (row, column): n1, n2 = n1 -+ 1, n3 = the partner's n2
+  const int va[3] = {even ? r : r + 1, even ? r : r + 1, even ? r + 1 : r};
+  const int vb[3] = {even ? j : j + 1, even ? j + 1 : j, even ? j : j + 1};
+  double v[6];
+  for (int k = 0; k < 3; ++k) grid_point(g, va[k], vb[k], &v[2 * k], &v[2 * k + 1]);
+  for (int k = 0; k < 6; ++k) verts[6ll * e + k] = v[k];
+  const double x0 = v[0], y0 = v[1], x1 = v[2], y1 = v[3], x2 = v[4], y2 = v[5];
+  const double j00 = x1 - x0, j01 = x2 - x0, j10 = y1 - y0, j11 = y2 - y0;
+  const double det = __dsub_rn(__dmul_rn(j00, j11), __dmul_rn(j10, j01));
+  const double rdet = 1 / det;
+  const double i00 = __dmul_rn(rdet, y2 - y0), i01 = __dmul_rn(rdet, x0 - x2);
+  const double i10 = __dmul_rn(rdet, y0 - y1), i11 = __dmul_rn(rdet, x1 - x0);
+  const double l0 = pow(__dadd_rn(__dmul_rn(x1 - x0, x1 - x0), __dmul_rn(y1 - y0, y1 - y0)), 0.5);
+  const double l1 = pow(__dadd_rn(__dmul_rn(x2 - x1, x2 - x1), __dmul_rn(y2 - y1, y2 - y1)), 0.5);
+  const double l2 = pow(__dadd_rn(__dmul_rn(x0 - x2, x0 - x2), __dmul_rn(y0 - y2, y0 - y2)), 0.5);
+  geo[0 * Kpad + e] = make_double2(i00, i01);
+  geo[1 * Kpad + e] = make_double2(i10, i11);
+  geo[2 * Kpad + e] = make_double2((y1 - y0) / l0, -1 * (x1 - x0) / l0);
+  geo[3 * Kpad + e] = make_double2((y2 - y1) / l1, -1 * (x2 - x1) / l1);
+  geo[4 * Kpad + e] = make_double2((y0 - y2) / l2, -1 * (x0 - x2) / l2);
+  geo[5 * Kpad + e] = make_double2(l0 / det, l1 / det);
+  geo[6 * Kpad + e] = make_double2(l2 / det, det);
+  const int left = e % (2 * nx) == 0 ? e - 1 + 2 * nx : e - 1;
+  const int right = (e + 1) % (2 * nx) == 0 ? e + 1 - 2 * nx : e + 1;
+  int vert;
+  if (e >= 2 * nx * (ny - 1)) vert = even ? e + 1 - 2 * nx : e - 1 - 2 * nx * (ny - 1);
+  else if (e >= 2 * nx) vert = even ? e + 1 - 2 * nx : e - 1 + 2 * nx;
+  else vert = even ? e + 1 + 2 * nx * (ny - 1) : e - 1 + 2 * nx;
+  nbr[e] = even ? make_int4(vert, right, left, 0) : make_int4(vert, left, right, 0);
+  if (!U) return;
+  for (int i = 0; i < Np; ++i) {  // nodal initial condition (Element.cpp:124-179)
+    const double xi = g.nodes_ref[2 * i], eta = g.nodes_ref[2 * i + 1], h0 = 1.0 - xi - eta;
+    double s4[4];
+    const double px = __dadd_rn(__dadd_rn(__dmul_rn(x0, h0), __dmul_rn(x1, xi)), __dmul_rn(x2, eta));
+    const double py = __dadd_rn(__dadd_rn(__dmul_rn(y0, h0), __dmul_rn(y1, xi)), __dmul_rn(y2, eta));
+    vortex_point(ic, px, py, 0.0, s4);
+    U[(2 * i) * Kpad + e] = make_double2(s4[0], s4[1]);
+    U[(2 * i + 1) * Kpad + e] = make_double2(s4[2], s4[3]);
+  }
+}
+
 __global__ void totals_final_kernel(const double* __restrict__ partial, int nblocks,
                                     double* __restrict__ out) {
   __shared__ double red[4][256];
@@ -486,6 +562,155 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
       release(c);
       return nullptr;
     }
+  }
+  set(VT_OK);
+  return c;
+}
+
+vt_ctx* vt_create_structured(const vt_params* prm, const vt_vortex* ic_in, int device, int* status) {
+  auto set = [&](int s) {
+    if (status) *status = s;
+  };
+  if (!prm) {
+    set(fail(VT_ERR_INVALID, "vt_create_structured: null parameters"));
+    return nullptr;
+  }
+  if (prm->p < 0 || prm->p > 3 || prm->integration_order < 0 || prm->integration_order > 19 ||
+      (prm->U_initialization_type != 0 && prm->U_initialization_type != 1)) {
+    set(fail(VT_ERR_UNSUPPORTED, "vt_create_structured: p, integration_order or U_initialization_type out of range"));
+    return nullptr;
+  }
+  const int nx = prm->num_element_in_x, ny = prm->num_element_in_y;
+  if (nx < 1 || ny < 1 || 2.0 * nx * ny > 2147483647.0 / 64) {
+    set(fail(VT_ERR_INVALID, "vt_create_structured: num_element_in_x/y out of range"));
+    return nullptr;
+  }
+  const vt_vortex ic = ic_in ? *ic_in : vt::default_vortex();
+  // reference-space tables (host, a few KB)
+  const int p = prm->p, Np = vt::np_of(p);
+  std::vector<double> line, area, minv, pp, pm;
+  vt::line_rule(prm->integration_order, &line);
+  vt::area_rule(prm->integration_order, &area);
+  const std::vector<double> nodes_ref = vt::reference_nodes(p);
+  if (!vt::inverse_mass_reference(p, area, &minv)) {
+    set(fail(VT_ERR_UNSUPPORTED, "vt_create_structured: the reference mass matrix is singular for this rule"));
+    return nullptr;
+  }
+  const std::vector<double> stiff = vt::stiffness_reference(p, area);
+  vt::face_tables(p, line, &pp, &pm);
+  const int nfq = static_cast<int>(line.size() / 2);
+  if (nfq < 1 || nfq > 10) {
+    set(fail(VT_ERR_UNSUPPORTED, "vt_create_structured: n_line_points must be 1..10"));
+    return nullptr;
+  }
+  cudaError_t e = cudaSetDevice(device);
+  if (e) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("cudaSetDevice", e)));
+    return nullptr;
+  }
+  auto* c = new vt_ctx();
+  c->device = device;
+  c->p = p;
+  c->Np = Np;
+  c->nfq = nfq;
+  c->K = 2 * nx * ny;
+  c->Kpad = (static_cast<long long>(c->K) + 127) / 128 * 128;
+  const vt::StageKernel sk = vt::select_kernel(p, nfq);
+  c->launch = sk.launch;
+  int per_sm = 0, sms = 0;
+  if ((e = sk.configure(&per_sm)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device))) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
+    delete c;
+    return nullptr;
+  }
+  c->max_blocks = sms * (per_sm > 0 ? per_sm : 1);
+  c->ops = vt::fold_operators(p, nfq, minv.data(), stiff.data(), line.data(), pp.data(), pm.data());
+  c->minv_ref = minv;
+  c->side_pairing = true;
+  std::vector<double> m(minv), W(Np, 0.0);
+  vt::invert_gauss_jordan(Np, &m);
+  for (int i = 0; i < Np; ++i)
+    for (int j = 0; j < Np; ++j) W[i] += m[i * Np + j];
+
+  const long long KP = c->Kpad;
+  const size_t state_bytes = sizeof(double2) * 2 * Np * static_cast<size_t>(KP);
+  const int tot_blocks = (c->K + 255) / 256;
+  double* verts = nullptr;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) || (e = alloc(&c->U, state_bytes)) ||
+      (e = alloc(&c->A, state_bytes)) || (e = alloc(&c->Sa, state_bytes)) || (e = alloc(&c->Sb, state_bytes)) ||
+      (e = alloc(&c->geo, sizeof(double2) * 7 * KP)) || (e = alloc(&c->nbr, sizeof(int4) * KP)) ||
+      (e = alloc(&c->err, 4 * sizeof(unsigned long long))) || (e = alloc(&c->W, sizeof(double) * Np)) ||
+      (e = alloc(&c->partial, sizeof(double) * 4 * tot_blocks)) || (e = alloc(&c->tot, sizeof(double) * 4)) ||
+      (e = alloc(&verts, sizeof(double) * 6 * static_cast<size_t>(c->K)))) {
+    set(fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, vt::cuda_msg("vt_create_structured", e)));
+    if (verts) cudaFree(verts);
+    release(c);
+    return nullptr;
+  }
+  // grid origin and spacing as the reference rounds them (float, then widened)
+  vt::GridSpec g{};
+  g.nx = nx;
+  g.ny = ny;
+  const float esxf = prm->domain_x / nx, esyf = prm->domain_y / ny;
+  const float gx0f = -1 * prm->domain_x / 2, gy0f = -1 * prm->domain_y / 2;
+  g.esx = esxf;
+  g.esy = esyf;
+  g.gx0 = gx0f;
+  g.gy0 = gy0f;
+  g.pg = prm->perturb_grid;
+  for (int i = 0; i < 2 * Np; ++i) g.nodes_ref[i] = nodes_ref[i];
+  // the projected initial condition's table: basis at the area points, weights, points, M_ref^-1
+  const int nq = static_cast<int>(area.size() / 3);
+  std::vector<double> tab(static_cast<size_t>(nq) * (Np + 3) + Np * Np);
+  for (int q = 0; q < nq; ++q) {
+    vt::basis(p, area[3 * q], area[3 * q + 1], &tab[static_cast<size_t>(q) * Np]);
+    tab[static_cast<size_t>(nq) * Np + q] = area[3 * q + 2];
+    tab[static_cast<size_t>(nq) * (Np + 1) + 2 * q] = area[3 * q];
+    tab[static_cast<size_t>(nq) * (Np + 1) + 2 * q + 1] = area[3 * q + 1];
+  }
+  std::copy(minv.begin(), minv.end(), tab.begin() + static_cast<size_t>(nq) * (Np + 3));
+  double* dtab = nullptr;
+  if (!e) e = cudaMemsetAsync(c->U, 0, state_bytes, c->stream);
+  if (!e) e = cudaMemsetAsync(c->A, 0, state_bytes, c->stream);
+  if (!e) e = cudaMemsetAsync(c->Sa, 0, state_bytes, c->stream);
+  if (!e) e = cudaMemsetAsync(c->Sb, 0, state_bytes, c->stream);
+  if (!e) e = cudaMemsetAsync(c->geo, 0, sizeof(double2) * 7 * KP, c->stream);
+  if (!e) e = cudaMemsetAsync(c->nbr, 0, sizeof(int4) * KP, c->stream);
+  if (!e) e = cudaMemcpyAsync(c->W, W.data(), sizeof(double) * Np, cudaMemcpyHostToDevice, c->stream);
+  if (!e) {
+    vt::structured_mesh_kernel<<<(c->K + 127) / 128, 128, 0, c->stream>>>(
+        g, Np, KP, verts, c->geo, c->nbr, ic, prm->U_initialization_type == 0 ? c->U : nullptr);
+    e = cudaGetLastError();
+  }
+  if (!e && prm->U_initialization_type == 1) {
+    e = alloc(&dtab, sizeof(double) * tab.size());
+    if (!e) e = cudaMemcpyAsync(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->stream);
+    if (!e) {
+      vt::project_vortex_kernel<<<(c->K + 127) / 128, 128, 0, c->stream>>>(verts, c->geo, dtab, nq, ic, 0.0, c->K, Np,
+                                                                          KP, c->U);
+      e = cudaGetLastError();
+    }
+  }
+  // tiles: two-row runs of the structured mesh, or runs of consecutive elements
+  const std::vector<int4> runs = vt::grid_tile_runs(nx, ny);
+  c->ntiles = runs.empty() ? (c->K + vt::kTileElems - 1) / vt::kTileElems : static_cast<int>(runs.size());
+  if (!e) e = alloc(&c->tiles, sizeof(int4) * c->ntiles);
+  if (!e) e = alloc(&c->tile_items, sizeof(int) * vt::kMaxItems * static_cast<size_t>(c->ntiles));
+  if (!e) e = alloc(&c->tile_count, sizeof(int) * c->ntiles);
+  if (!e) {
+    if (runs.empty())
+      e = vt::launch_contiguous_tiles(c->tiles, c->K, c->ntiles, c->stream);
+    else
+      e = cudaMemcpyAsync(c->tiles, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice, c->stream);
+  }
+  if (!e) e = vt::launch_build_tile_items(c->tiles, c->nbr, c->tile_items, c->tile_count, c->ntiles, c->stream);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  cudaFree(verts);
+  if (dtab) cudaFree(dtab);
+  if (e) {
+    set(fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, vt::cuda_msg("vt_create_structured", e)));
+    release(c);
+    return nullptr;
   }
   set(VT_OK);
   return c;
