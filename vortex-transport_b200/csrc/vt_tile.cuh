@@ -27,9 +27,7 @@
 //   5. flux   the nodal Euler flux of every node, contracted with the inverse
 //             Jacobian, once, into shared memory; the state tile is then free
 //             and the next tile's copies are issued;
-//   6. volume D_xi G_xi + D_eta G_eta per component; the element's four
-//             accumulators then meet in shared memory and the RK stage update
-//             is written back as whole double2 rows (full sectors per warp).
+//   6. volume D_xi G_xi + D_eta G_eta, then the RK stage update written back.
 //
 // Upcoming rows are also prefetched into L2 (cp.async.bulk.prefetch.L2) one
 // tile ahead and the tile's geometry rows into L1, so no phase waits on HBM.
@@ -116,8 +114,6 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 constexpr unsigned kMaxWaitTries = 1u << 22;
-// resident blocks per SM the shared-memory tile allows (about 73 KB per 64 elements at p = 3)
-constexpr int kStageBlocksPerSM = 3 * 64 / kTileElems;
 
 // Warp 0 issues the bulk copies of a tile's 2*Np state rows (two runs each)
 // into S, after lane 0 announced the byte count on the barrier.
@@ -141,7 +137,7 @@ __device__ __forceinline__ void issue_tile_copies(const StageArgs& a, const int4
 template <int P, int NFQ>
 // Three 256-thread blocks per SM (<= 80 registers per thread) keep 24 warps
 // resident alongside 3 x ~75 KB of shared memory.
-__global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_kernel(const StageArgs a,
+__global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const StageArgs a,
                                                                         const StageOps<P, NFQ> ops) {
   using L = TileLayout<P, NFQ>;
   constexpr int E = L::E;
@@ -177,13 +173,12 @@ __global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_
   __syncthreads();
 
   // tile metadata of the tile in hand: run, face count, this thread's face
-  // item (slots past the count are read but not used), this column's
-  // neighbours and side-0 neighbour rows
+  // item, this column's neighbours and side-0 neighbour rows
   int tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   int4 run = __ldg(a.tiles + tile);
   int nitems = __ldg(a.tile_count + tile);
-  int my_item = t < kMaxItems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
+  int my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
   int4 my_nb = make_int4(0, 0, 0, 0);
   double2 hreg[2];
   {
@@ -205,21 +200,20 @@ __global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_
 
     // ---- prefetch: the next tile into L2 (its state copies start in phase 5), this
     // tile's RK rows into L2 and its geometry rows into L1 -----------------------
-    if (has_next) {  // next tile: 2 Np state rows, 7 geometry rows and the neighbour row, two runs each
-      const int4 rr = __ldg(a.tiles + tile + G);
-      for (int l = t; l < 2 * (2 * NP + 8); l += T) {
-        const int which = l & 1, r = l >> 1;
+    if (t < 64) {
+      if (has_next) {
+        const int4 rr = __ldg(a.tiles + tile + G);
+        const int which = t & 1, r = t >> 1;
         const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
         if (len > 0) {
           const unsigned bytes = static_cast<unsigned>(len) * 16u;
           if (r < 2 * NP) prefetch_l2(a.in + r * KP + start, bytes);
           else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
-          else prefetch_l2(a.nbr + start, bytes);
+          else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
         }
       }
-    }
-    for (int l = t; l < 2 * 4 * NP; l += T) {  // this tile's RK accumulator and base rows
-      const int which = l & 1, r = l >> 1;
+    } else if (t < 64 + 8 * NP) {
+      const int l = t - 64, which = l & 1, r = l >> 1;
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
       if (len > 0) {
         const unsigned bytes = static_cast<unsigned>(len) * 16u;
@@ -229,14 +223,11 @@ __global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_
           prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
         }
       }
-    }
-    {  // this tile's 7 geometry rows into L1 (128-byte lines, kTileRun / 8 per run)
-      constexpr int LPR = kTileRun / 8;
-      for (int l = t; l < 7 * 2 * LPR; l += T) {
-        const int row = l / (2 * LPR), which = (l / LPR) & 1, line = l % LPR;
-        const int start = which ? run.z : run.x, len = which ? run.w : run.y;
-        if (line * 8 < len) prefetch_l1(a.geo + row * KP + start + line * 8);
-      }
+    } else if (t < 64 + 8 * NP + 56) {
+      // this tile's 7 geometry rows into L1 (4 lines per 32-element run)
+      const int l = t - 64 - 8 * NP, row = l >> 3, which = (l >> 2) & 1, line = l & 3;
+      const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+      if (line * 8 < len) prefetch_l1(a.geo + row * KP + start + line * 8);
     }
 
     // ---- 1. load ------------------------------------------------------------------
@@ -342,7 +333,7 @@ __global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_
     // next tile's metadata (next_run has arrived by now)
     if (has_next) {
       nitems = __ldg(a.tile_count + tile + G);
-      my_item = t < kMaxItems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
+      my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       my_nb = pos < (second ? next_run.w : next_run.y) ? __ldg(a.nbr + (second ? next_run.z : next_run.x) + pos)
@@ -417,52 +408,46 @@ __global__ void __launch_bounds__(4 * kTileElems, kStageBlocksPerSM) tile_stage_
       }
     }
 
-    // ---- 6b. stage update -------------------------------------------------------------
-    // The four component accumulators of each element meet in shared memory
-    // (the flux buffer is free once every thread has finished the volume term);
-    // then thread (element, pair h, node parity) reads and writes whole double2
-    // rows, so each warp request covers full 32-byte sectors.
-    __syncthreads();
-    double* Rs = FB;  // [NP][4][ES]
-#pragma unroll
-    for (int i = 0; i < NP; ++i) Rs[(i * 4 + c) * ES + el] = r[i];
-    __syncthreads();
+    // ---- 6b. stage update: component c of every node ----------------------------------
     if (valid) {
       const double dtt = a.tile_dt ? __ldg(a.tile_dt + tile) : 1.0;
       const double c_acc = a.c_acc * dtt, c_out = a.c_out * dtt;
-      const int h = grp & 1, first = grp >> 1;  // pair and node parity of this thread
+      const int h = c >> 1, part = c & 1;
+      const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
+      const double* in = reinterpret_cast<const double*>(a.in) + off0;
+      const double* base = reinterpret_cast<const double*>(a.base) + off0;
+      double* acc = reinterpret_cast<double*>(a.acc) + off0;
+      double* out = reinterpret_cast<double*>(a.out) + off0;
+      const long long step = 4 * KP;  // doubles between node rows of the same pair
+      switch (a.stage) {
+        case 0:
 #pragma unroll
-      for (int i = first; i < NP; i += 2) {
-        const double2 ri = make_double2(Rs[(i * 4 + 2 * h) * ES + el], Rs[(i * 4 + 2 * h + 1) * ES + el]);
-        const long long idx = (2 * i + h) * KP + e;
-        switch (a.stage) {
-          case 0: {
-            const double2 u = __ldg(a.in + idx);
-            a.acc[idx] = make_double2(fma(c_acc, ri.x, u.x), fma(c_acc, ri.y, u.y));
-            a.out[idx] = make_double2(fma(c_out, ri.x, u.x), fma(c_out, ri.y, u.y));
-            break;
+          for (int i = 0; i < NP; ++i) {
+            const double u = __ldg(in + i * step);
+            acc[i * step] = fma(c_acc, r[i], u);
+            out[i * step] = fma(c_out, r[i], u);
           }
-          case 1:
-          case 2: {
-            const double2 ac = a.acc[idx], b = __ldg(a.base + idx);
-            a.acc[idx] = make_double2(fma(c_acc, ri.x, ac.x), fma(c_acc, ri.y, ac.y));
-            a.out[idx] = make_double2(fma(c_out, ri.x, b.x), fma(c_out, ri.y, b.y));
-            break;
+          break;
+        case 1:
+        case 2:
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            acc[i * step] = fma(c_acc, r[i], acc[i * step]);
+            out[i * step] = fma(c_out, r[i], __ldg(base + i * step));
           }
-          case 3: {
-            const double2 ac = a.acc[idx];
-            a.out[idx] = make_double2(fma(c_out, ri.x, ac.x), fma(c_out, ri.y, ac.y));
-            break;
-          }
-          case kStageEuler: {
-            const double2 u = __ldg(a.in + idx);
-            a.out[idx] = make_double2(fma(c_out, ri.x, u.x), fma(c_out, ri.y, u.y));
-            break;
-          }
-          default:
-            a.out[idx] = ri;
-            break;
-        }
+          break;
+        case 3:
+#pragma unroll
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], acc[i * step]);
+          break;
+        case kStageEuler:
+#pragma unroll
+          for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], __ldg(in + i * step));
+          break;
+        default:
+#pragma unroll
+          for (int i = 0; i < NP; ++i) out[i * step] = r[i];
+          break;
       }
     }
     run = next_run;
