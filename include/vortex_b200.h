@@ -328,9 +328,9 @@ void vt_roe_flux_vjp(const double* uL, const double* uR, double nx, double ny, c
 
 /* Adjoint of a batched run: vt_adjoint_forward / vt_adjoint_backward over each
  * group's ragged element array (one launch per stage for all instances of a
- * group; the instances of a group must share one time step, set by
- * vt_batch_set_dt). dJdU_T and dJdU_0 are host arrays holding every instance's
- * K_i x Np_i x 4 block, in instance order. */
+ * group, each instance with its own time step from vt_batch_set_dt). dJdU_T
+ * and dJdU_0 are host arrays holding every instance's K_i x Np_i x 4 block, in
+ * instance order. */
 int vt_batch_adjoint_forward(vt_batch* batch, int nsteps, int nsnapshots);
 int vt_batch_adjoint_backward(vt_batch* batch, const double* dJdU_T, double* dJdU_0);
 int vt_batch_adjoint_info(const vt_batch* batch, int group, vt_checkpoint_info* out);

@@ -130,8 +130,9 @@ def test_rhs_jvp_matches_central_differences(vt, nx, ny, p, io):
     np.testing.assert_allclose(JV, fd, rtol=0, atol=1e-7 * np.abs(fd).max())
 
 
-def test_tangent_adjoint_dot_product_and_checkpoints(vt):
-    pb = problem(vt, 16, 16, 3, 10)
+@pytest.mark.parametrize("p,io", [(3, 10), (2, 6), (1, 4)])
+def test_tangent_adjoint_dot_product_and_checkpoints(vt, p, io):
+    pb = problem(vt, 16, 16, p, io)
     dt, n = 1e-3, 24
     U0 = pb.array("U0")
     rng = np.random.default_rng(5)
@@ -160,9 +161,10 @@ def test_tangent_adjoint_dot_product_and_checkpoints(vt):
     assert rel(np.sum(lT * dT), np.sum(lams[0] * d0)) < DOT_RTOL
 
 
-def test_state_gradient_matches_central_differences(vt):
-    pb = problem(vt, 16, 16, 3, 10)
-    target_pb = problem(vt, 16, 16, 3, 10, epsilon=0.35, x0=0.4, y0=-0.25)
+@pytest.mark.parametrize("p,io", [(3, 10), (2, 6), (1, 4)])
+def test_state_gradient_matches_central_differences(vt, p, io):
+    pb = problem(vt, 16, 16, p, io)
+    target_pb = problem(vt, 16, 16, p, io, epsilon=0.35, x0=0.4, y0=-0.25)
     dt, n = 1e-3, 40
     J, dJ = mass_loss(pb)
     t = vt.Solver(target_pb)

@@ -253,8 +253,13 @@ cudaError_t stage(vt_ctx* c, const double2* in, const double2* base, double2* ou
   return c->launch(stage_args(c, in, base, c->A, out, st, ca, co), c->ops.data(), c->max_blocks, c->stream);
 }
 
+// The step size the coefficients carry: dt, or 1 when the device scales them
+// by each tile's / element's own time step (a batch group).
+double dt_scale(const vt_ctx* c, double dt) { return c->tile_dt ? 1.0 : dt; }
+
 // One plain RK4 step from X into Y (Y may be X), stages through Sa, Sb.
-cudaError_t plain_step(vt_ctx* c, const double2* X, double2* Y, double dt) {
+cudaError_t plain_step(vt_ctx* c, const double2* X, double2* Y, double dt0) {
+  const double dt = dt_scale(c, dt0);
   cudaError_t e;
   if ((e = stage(c, X, X, c->Sa, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
   if ((e = stage(c, c->Sa, X, c->Sb, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
@@ -270,8 +275,9 @@ cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt) {
 
 // Step from X keeping the stage states in S1, S2, S3; the new state goes to
 // `out` when given (else the last stage is not run).
-cudaError_t stage_step(vt_ctx* c, const double2* X, double2* S1, double2* S2, double2* S3, double dt,
+cudaError_t stage_step(vt_ctx* c, const double2* X, double2* S1, double2* S2, double2* S3, double dt0,
                        double2* out) {
+  const double dt = dt_scale(c, dt0);
   cudaError_t e;
   if ((e = stage(c, X, X, S1, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
   if ((e = stage(c, S1, X, S2, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
@@ -287,6 +293,7 @@ AdjArgs adj_args(vt_ctx* c) {
   AdjArgs a{};
   a.bp = c->adj->bp;
   a.bm = c->adj->bm;
+  a.elem_dt = c->elem_dt;
   a.owners = c->adj->owners;
   a.owner_nb = c->adj->owner_nb;
   a.is_owner = c->adj->is_owner;
@@ -306,14 +313,15 @@ cudaError_t reverse_stage(vt_ctx* c, const AdjArgs& a) {
 
 // lam <- adjoint of U_i given lam = adjoint of U_{i+1}; X = U_i, stage states S1..S3.
 cudaError_t adjoint_step(vt_ctx* c, const double2* X, const double2* S1, const double2* S2, const double2* S3,
-                         double dt) {
+                         double dt0) {
   AdjointState* s = c->adj;
+  const double dt = dt_scale(c, dt0);
   AdjArgs a = adj_args(c);
   cudaError_t e;
-  a.U = S3, a.a = s->lam, a.sa = (1.0 / 6) * dt, a.lam = s->lam, a.acc_in = nullptr, a.lam_coef = 1.0;
+  a.U = S3, a.a = s->lam, a.sa = (1.0 / 6) * dt, a.sa_dt = 1, a.lam = s->lam, a.acc_in = nullptr, a.lam_coef = 1.0;
   a.acc_out = s->acc, a.a_out = s->a1, a.cl = (1.0 / 3) * dt, a.cg = dt;
   if ((e = reverse_stage(c, a))) return e;
-  a.U = S2, a.a = s->a1, a.sa = 1.0, a.acc_in = s->acc, a.lam_coef = 0.0;
+  a.U = S2, a.a = s->a1, a.sa = 1.0, a.sa_dt = 0, a.acc_in = s->acc, a.lam_coef = 0.0;
   a.acc_out = s->acc, a.a_out = s->a0, a.cl = (1.0 / 3) * dt, a.cg = 0.5 * dt;
   if ((e = reverse_stage(c, a))) return e;
   a.U = S1, a.a = s->a0, a.a_out = s->a1, a.cl = (1.0 / 6) * dt, a.cg = 0.5 * dt;

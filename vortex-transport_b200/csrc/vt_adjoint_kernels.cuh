@@ -54,6 +54,10 @@ struct AdjArgs {
   const int* owner_nb;              // [3][nowners]: each owner's neighbour across side s
   const unsigned char* is_owner;    // K flags, or null
   int nowners;
+  // Per-element time steps (a batch group with uneven steps), or null: then
+  // sa (when sa_dt is set), cl and cg are fractions of the element's step.
+  const double* elem_dt;
+  int sa_dt;
   long long Kpad;
   int K;
   double sa, lam_coef, cl, cg;
@@ -99,7 +103,8 @@ __global__ void __launch_bounds__(kAdjRun * NFQ)
     bf[3] = fma(l, a1.y, bf[3]);
   }
   const double2 lsa = __ldg(a.geo + 5 * KP + e), lsb = __ldg(a.geo + 6 * KP + e);
-  const double sc = -(s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x)) * a.sa;
+  const double sa = (a.elem_dt && a.sa_dt) ? a.sa * __ldg(a.elem_dt + e) : a.sa;
+  const double sc = -(s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x)) * sa;
 #pragma unroll
   for (int c = 0; c < 4; ++c) bf[c] *= sc;
   const double2 n = __ldg(a.geo + (2 + s) * KP + e);
@@ -190,8 +195,9 @@ __global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 4 : 2)
   }
   const double2 lea = sh[RG][lane], leb = sh[RG + 1][lane];
   const double2 lna = sh[RG + 2][lane], lnb = sh[RG + 3][lane];
-  const double se = -(s == 0 ? lea.x : (s == 1 ? lea.y : leb.x)) * a.sa;
-  const double sn = (s == 0 ? lna.x : (s == 1 ? lna.y : lnb.x)) * a.sa;
+  const double sa = (a.elem_dt && a.sa_dt) ? a.sa * __ldg(a.elem_dt + e) : a.sa;  // nb: same instance
+  const double se = -(s == 0 ? lea.x : (s == 1 ? lea.y : leb.x)) * sa;
+  const double sn = (s == 0 ? lna.x : (s == 1 ? lna.y : lnb.x)) * sa;
   double bf[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) bf[c] = fma(se, be[c], sn * bn[c]);
@@ -253,10 +259,11 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P), 3)
       by[2] = fma(d1, a1.x, by[2]);
       by[3] = fma(d1, a1.y, by[3]);
     }
+    const double sa = (a.elem_dt && a.sa_dt) ? a.sa * __ldg(a.elem_dt + e) : a.sa;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      bx[c] *= a.sa;
-      by[c] *= a.sa;
+      bx[c] *= sa;
+      by[c] *= sa;
     }
     const double sv[4] = {u0.x, u0.y, u1.x, u1.y};
     contravariant_vjp(sv, j0.x, j0.y, j1.x, j1.y, bx, by, g);
@@ -298,9 +305,11 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P), 3)
 #pragma unroll
   for (int c = 0; c < 4; ++c) acc[c] = fma(a.lam_coef, lam[c], acc[c]) + g[c];
   if (a.a_out) {
+    const double h = a.elem_dt ? __ldg(a.elem_dt + e) : 1.0;
+    const double cl = a.elem_dt ? a.cl * h : a.cl, cg = a.elem_dt ? a.cg * h : a.cg;
     double an[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) an[c] = fma(a.cl, lam[c], a.cg * g[c]);
+    for (int c = 0; c < 4; ++c) an[c] = fma(cl, lam[c], cg * g[c]);
     a.a_out[r0] = make_double2(an[0], an[1]);
     a.a_out[r1] = make_double2(an[2], an[3]);
   }

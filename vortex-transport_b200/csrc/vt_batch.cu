@@ -126,8 +126,10 @@ struct vt_batch {
   std::vector<double> dt;  // per instance
   int last_instance = -1;
   vt_error_info last{};
-  // one solver context per group over the group's own buffers, for the adjoint
+  // one solver context per group over the group's own buffers, for the adjoint,
+  // with each group's per-element time steps
   std::vector<vt_ctx*> views;
+  std::vector<double*> view_dt;
 };
 
 namespace {
@@ -142,6 +144,8 @@ void release(vt_batch* b) {
     if (v->aos) cudaFree(v->aos);
     delete v;
   }
+  for (double* p : b->view_dt)
+    if (p) cudaFree(p);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (auto& g : b->groups) {
     void* bufs[] = {g.U, g.A, g.Sa, g.Sb, g.geo, g.nbr, g.tiles, g.items, g.count, g.tile_dt, g.err};
@@ -263,6 +267,16 @@ int ensure_views(vt_batch* b) {
     c->err = G.err;
     c->ops = G.ops;
     c->launch = G.kern.launch;
+    c->tile_dt = G.tile_dt;
+    double* edt = nullptr;
+    const cudaError_t ea = cudaMalloc(reinterpret_cast<void**>(&edt), sizeof(double) * static_cast<size_t>(G.K));
+    if (ea) {
+      delete c;
+      return fail(ea == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA,
+                  vt::cuda_msg("batch adjoint set-up", ea));
+    }
+    c->elem_dt = edt;
+    b->view_dt.push_back(edt);
     std::vector<int4> nb(static_cast<size_t>(G.K));
     const cudaError_t e = cudaMemcpy(nb.data(), G.nbr, sizeof(int4) * nb.size(), cudaMemcpyDeviceToHost);
     if (e) {
@@ -543,13 +557,17 @@ int vt_batch_adjoint_forward(vt_batch* b, int nsteps, int nsnapshots) {
   b->last_instance = -1;
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     vt::Group& G = b->groups[gi];
-    const double dt = b->dt[G.members[0]];
-    for (int m : G.members)
-      if (b->dt[m] != dt)
-        return fail(VT_ERR_UNSUPPORTED, "vt_batch_adjoint_forward: the instances of a group need one time step");
     vt_ctx* c = b->views[gi];
+    // each element steps with its instance's time step (the tiles already carry it)
+    std::vector<double> edt(static_cast<size_t>(G.K));
+    for (size_t m = 0; m < G.members.size(); ++m)
+      std::fill(edt.begin() + G.offset[m], edt.begin() + G.offset[m] + b->K_of[G.members[m]], b->dt[G.members[m]]);
+    cudaError_t e = cudaMemcpyAsync(b->view_dt[gi], edt.data(), sizeof(double) * edt.size(), cudaMemcpyHostToDevice,
+                                    b->stream);
+    if (!e) e = cudaStreamSynchronize(b->stream);
+    if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("batch adjoint time steps", e));
     c->max_blocks = G.max_blocks;
-    st = vt_adjoint_forward(c, dt, nsteps, nsnapshots);
+    st = vt_adjoint_forward(c, 1.0, nsteps, nsnapshots);
     if (st > 0) {  // map the group element to its instance
       vt_error_info info{};
       vt_last_error(c, &info);

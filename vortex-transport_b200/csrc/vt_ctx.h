@@ -41,6 +41,10 @@ struct vt_ctx {
   int pending_steps = 0;
   double pending_dt = 0.0;
   bool side_pairing = false;  // nbr(nbr(e, s), s) == e for every element and side
+  // Per-tile / per-element time steps (a batch group's view; null otherwise):
+  // stage and adjoint coefficients are then fractions scaled on the device.
+  const double* tile_dt = nullptr;
+  const double* elem_dt = nullptr;
   vt::AdjointState* adj = nullptr;
 };
 

@@ -347,7 +347,7 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
   a.nbr = c->nbr;
   a.tiles = c->tiles;
   a.tile_items = c->tile_items;
-  a.tile_dt = nullptr;
+  a.tile_dt = c->tile_dt;
   a.tile_count = c->tile_count;
   a.ntiles = c->ntiles;
   a.err = c->err;
