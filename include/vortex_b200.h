@@ -251,6 +251,9 @@ int vt_batch_group_info(const vt_batch* batch, int group, int* p, int* n_instanc
 /* Per-instance state transfer, host arrays in the reference layout. */
 int vt_batch_upload_state(vt_batch* batch, int instance, const double* U);
 int vt_batch_download_state(vt_batch* batch, int instance, double* U, double* F);
+/* The same with U a device array (K_i x Np_i x 4) on the batch's device. */
+int vt_batch_upload_state_device(vt_batch* batch, int instance, const double* dU);
+int vt_batch_download_state_device(vt_batch* batch, int instance, double* dU);
 /* Per-instance time steps, dt[n]. */
 int vt_batch_set_dt(vt_batch* batch, const double* dt);
 /* nsteps RK4 steps of every instance; blocks until done. A non-physical state
@@ -333,6 +336,8 @@ void vt_roe_flux_vjp(const double* uL, const double* uR, double nx, double ny, c
  * instance order. */
 int vt_batch_adjoint_forward(vt_batch* batch, int nsteps, int nsnapshots);
 int vt_batch_adjoint_backward(vt_batch* batch, const double* dJdU_T, double* dJdU_0);
+/* The same with dJdU_T / dJdU_0 in device memory. */
+int vt_batch_adjoint_backward_device(vt_batch* batch, const double* dJdU_T, double* dJdU_0);
 int vt_batch_adjoint_info(const vt_batch* batch, int group, vt_checkpoint_info* out);
 
 /* ---- stepping without device allocation --------------------------------- */

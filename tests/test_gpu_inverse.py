@@ -27,6 +27,13 @@ def test_batch_adjoint_matches_single_solver(vt, dts):
     lams = [rng.standard_normal((pb.K, pb.Np, 4)) for pb in pbs]
     got = batch.adjoint_backward(lams)
     assert batch.adjoint_info()["advance_steps"] == batch.adjoint_info()["optimal_advance_steps"]
+    import torch
+    on_device = batch.adjoint_backward([torch.tensor(x, device="cuda") for x in lams])  # device-pointer path
+    for i in range(len(pbs)):
+        np.testing.assert_array_equal(on_device[i].cpu().numpy(), got[i])
+        U = torch.empty((pbs[i].K, pbs[i].Np, 4), dtype=torch.float64, device="cuda")
+        batch.download_device(i, U)
+        np.testing.assert_array_equal(U.cpu().numpy(), batch.download(i))
     for i, pb in enumerate(pbs):
         s = vt.Solver(pb)
         s.adjoint_forward(dts[i], n, 8)

@@ -193,6 +193,9 @@ _SIGNATURES = {
     "vt_roe_flux_vjp": (None, [_dp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]),
     "vt_batch_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "vt_batch_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "vt_batch_adjoint_backward_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "vt_batch_upload_state_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "vt_batch_download_state_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "vt_batch_adjoint_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "vt_noalloc_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     "vt_step_rk4_noalloc": (ctypes.c_int, [ctypes.POINTER(vt_device_mesh), ctypes.c_void_p,
@@ -699,6 +702,18 @@ class Batch:
         _check(lib().vt_batch_download_state(self._h, i, U.ctypes.data_as(ctypes.c_void_p), None))
         return U
 
+    def upload_device(self, i: int, U) -> None:
+        """Instance i's state from a CUDA float64 tensor (K_i, Np_i, 4) on the batch's device."""
+        assert tuple(U.shape) == (*self.shapes[i], 4) and U.is_contiguous()
+        import torch
+        torch.cuda.current_stream(U.device).synchronize()
+        _check(lib().vt_batch_upload_state_device(self._h, i, ctypes.c_void_p(U.data_ptr())))
+
+    def download_device(self, i: int, out) -> None:
+        """Instance i's state into a CUDA float64 tensor (K_i, Np_i, 4)."""
+        assert tuple(out.shape) == (*self.shapes[i], 4) and out.is_contiguous()
+        _check(lib().vt_batch_download_state_device(self._h, i, ctypes.c_void_p(out.data_ptr())))
+
     def set_dt(self, dt) -> None:
         dt = np.ascontiguousarray(dt, dtype=np.float64)
         assert dt.shape == (self.n,)
@@ -722,8 +737,21 @@ class Batch:
         of a group share one time step)."""
         self._status(lib().vt_batch_adjoint_forward(self._h, int(nsteps), int(nsnapshots)))
 
-    def adjoint_backward(self, dJdU_T) -> list[np.ndarray]:
-        """dJ/dU(0) per instance from dJ/dU(T) per instance (lists of (K_i, Np_i, 4))."""
+    def adjoint_backward(self, dJdU_T) -> list:
+        """dJ/dU(0) per instance from dJ/dU(T) per instance (lists of (K_i, Np_i, 4)
+        numpy arrays, or CUDA tensors: then the result is CUDA tensors too)."""
+        if _is_cuda_tensor(dJdU_T[0]):
+            import torch
+            flat = torch.cat([t.reshape(-1) for t in dJdU_T]).to(torch.float64).contiguous()
+            torch.cuda.current_stream(flat.device).synchronize()
+            out = torch.empty_like(flat)
+            _check(lib().vt_batch_adjoint_backward_device(self._h, ctypes.c_void_p(flat.data_ptr()),
+                                                          ctypes.c_void_p(out.data_ptr())))
+            res, o = [], 0
+            for K, Np in self.shapes:
+                res.append(out[o:o + K * Np * 4].view(K, Np, 4))
+                o += K * Np * 4
+            return res
         flat = np.concatenate([np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in dJdU_T])
         assert flat.size == sum(K * Np * 4 for K, Np in self.shapes)
         out = np.empty_like(flat)

@@ -491,6 +491,34 @@ int vt_batch_download_state(vt_batch* b, int i, double* U, double* F) {
   return VT_OK;
 }
 
+int vt_batch_upload_state_device(vt_batch* b, int i, const double* dU) {
+  if (!b || !dU || i < 0 || i >= b->n) return fail(VT_ERR_INVALID, "vt_batch_upload_state_device: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  vt::Group& G = b->groups[b->group_of[i]];
+  const int K = b->K_of[i];
+  const long long nrow = static_cast<long long>(K) * 2 * G.Np;
+  vt::batch_aos_to_soa<<<static_cast<int>((nrow + 255) / 256), 256, 0, b->stream>>>(
+      reinterpret_cast<const double2*>(dU), G.U, K, G.Np, G.Kpad, G.offset[b->index_in_group[i]]);
+  cudaError_t e = cudaGetLastError();
+  if (!e) e = cudaStreamSynchronize(b->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_upload_state_device", e)) : VT_OK;
+}
+
+int vt_batch_download_state_device(vt_batch* b, int i, double* dU) {
+  if (!b || !dU || i < 0 || i >= b->n) return fail(VT_ERR_INVALID, "vt_batch_download_state_device: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  vt::Group& G = b->groups[b->group_of[i]];
+  const int K = b->K_of[i];
+  const long long nrow = static_cast<long long>(K) * 2 * G.Np;
+  vt::batch_soa_to_aos<<<static_cast<int>((nrow + 255) / 256), 256, 0, b->stream>>>(
+      G.U, reinterpret_cast<double2*>(dU), K, G.Np, G.Kpad, G.offset[b->index_in_group[i]]);
+  cudaError_t e = cudaGetLastError();
+  if (!e) e = cudaStreamSynchronize(b->stream);
+  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_download_state_device", e)) : VT_OK;
+}
+
 int vt_batch_set_dt(vt_batch* b, const double* dt) {
   if (!b || !dt) return fail(VT_ERR_INVALID, "vt_batch_set_dt: bad argument");
   std::lock_guard<std::mutex> lk(b->mu);
@@ -584,7 +612,19 @@ int vt_batch_adjoint_forward(vt_batch* b, int nsteps, int nsnapshots) {
   return VT_OK;
 }
 
+// Reverse sweep of every group; the instances' blocks are gathered into group
+// order (host arrays, or device arrays when device_pointers is set).
+static int batch_backward(vt_batch* b, const double* dJdU_T, double* dJdU_0, int device_pointers);
+
 int vt_batch_adjoint_backward(vt_batch* b, const double* dJdU_T, double* dJdU_0) {
+  return batch_backward(b, dJdU_T, dJdU_0, 0);
+}
+
+int vt_batch_adjoint_backward_device(vt_batch* b, const double* dJdU_T, double* dJdU_0) {
+  return batch_backward(b, dJdU_T, dJdU_0, 1);
+}
+
+static int batch_backward(vt_batch* b, const double* dJdU_T, double* dJdU_0, int device_pointers) {
   if (!b || !dJdU_T || !dJdU_0) return fail(VT_ERR_INVALID, "vt_batch_adjoint_backward: null argument");
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
@@ -596,6 +636,31 @@ int vt_batch_adjoint_backward(vt_batch* b, const double* dJdU_T, double* dJdU_0)
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     vt::Group& G = b->groups[gi];
     const size_t per = 4 * static_cast<size_t>(G.Np);
+    if (device_pointers) {
+      // group-order device buffers: the view's staging array and a scratch copy
+      double *din = nullptr, *dout = nullptr;
+      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&din), 2 * sizeof(double) * per * G.K);
+      if (e) return fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, vt::cuda_msg("batch adjoint", e));
+      dout = din + per * G.K;
+      for (size_t m = 0; m < G.members.size() && !e; ++m) {
+        const int i = G.members[m];
+        e = cudaMemcpyAsync(din + per * G.offset[m], dJdU_T + off[i], sizeof(double) * (off[i + 1] - off[i]),
+                            cudaMemcpyDeviceToDevice, b->stream);
+      }
+      if (!e) e = cudaStreamSynchronize(b->stream);
+      int st = e ? fail(VT_ERR_CUDA, vt::cuda_msg("batch adjoint gather", e)) : VT_OK;
+      if (!st) st = vt_adjoint_backward(b->views[gi], din, dout, 1);
+      for (size_t m = 0; m < G.members.size() && !st && !e; ++m) {
+        const int i = G.members[m];
+        e = cudaMemcpyAsync(dJdU_0 + off[i], dout + per * G.offset[m], sizeof(double) * (off[i + 1] - off[i]),
+                            cudaMemcpyDeviceToDevice, b->stream);
+      }
+      if (!st && !e) e = cudaStreamSynchronize(b->stream);
+      cudaFree(din);
+      if (st) return st;
+      if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("batch adjoint scatter", e));
+      continue;
+    }
     gin.resize(per * G.K);
     gout.resize(per * G.K);
     for (size_t m = 0; m < G.members.size(); ++m) {

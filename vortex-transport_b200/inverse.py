@@ -74,16 +74,23 @@ class BatchedInverse:
         with torch.no_grad():
             self._upload(self._ic(torch.tensor(self.theta_true, device=self.dev)))
         self.batch.rk4(steps)
-        self.target = torch.stack([torch.tensor(self.batch.download(i), device=self.dev) for i in range(self.n)])
+        self.target = self._download()
 
     def _ic(self, th: torch.Tensor) -> torch.Tensor:
         c = [th[:, k, None, None] for k in range(4)]
         return vortex_ic(self.nodes[None], c[0], c[1], c[2], c[3])
 
     def _upload(self, U0: torch.Tensor) -> None:
-        host = U0.detach().cpu().numpy()
+        U0 = U0.detach().contiguous()
         for i in range(self.n):
-            self.batch.upload(i, host[i])
+            self.batch.upload_device(i, U0[i])
+
+    def _download(self) -> torch.Tensor:
+        K, Np = self.batch.shapes[0]
+        out = torch.empty((self.n, K, Np, 4), dtype=torch.float64, device=self.dev)
+        for i in range(self.n):
+            self.batch.download_device(i, out[i])
+        return out
 
     def loss_and_grad(self, theta: np.ndarray):
         """Per-instance losses (n,) and gradients (n, 4) at theta (n, 4)."""
@@ -92,15 +99,16 @@ class BatchedInverse:
         t0 = time.perf_counter()
         self._upload(U0)
         self.batch.adjoint_forward(self.steps, self.nsnapshots)
-        UT = torch.stack([torch.tensor(self.batch.download(i), device=self.dev) for i in range(self.n)])
+        UT = self._download()
         d = UT - self.target
         Md = torch.einsum("ij,nejc->neic", self.M, d)
         w = self.detj[None, :, None, None]
         J = 0.5 * torch.sum(w * d * Md, dim=(1, 2, 3))
-        lam = self.batch.adjoint_backward([(w * Md)[i].cpu().numpy() for i in range(self.n)])
+        gT = (w * Md).contiguous()
+        lam = self.batch.adjoint_backward([gT[i] for i in range(self.n)])
         self.gpu_seconds += time.perf_counter() - t0
         self.evaluations += 1
-        g, = torch.autograd.grad(U0, th, grad_outputs=torch.tensor(np.stack(lam), device=self.dev))
+        g, = torch.autograd.grad(U0, th, grad_outputs=torch.stack(lam))
         return J.detach().cpu().numpy(), g.cpu().numpy()
 
     def gauss_newton_diagonal(self, theta: np.ndarray) -> np.ndarray:
