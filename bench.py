@@ -11,8 +11,9 @@ through one RK stage, so a step is K*Np*4 DOF-stages.
 --impl reference times the reference's own CPU code (oracle/_ref, the
 reference compiled from its sources with -O2 -fopenmp) with all host threads on
 a bounded sample of the same per-element work. With N>1 (torchrun) every rank
-advances its own replica (the problem does not need a collective); rank 0
-prints one JSON line.
+advances its own replica of the headline problem (it needs no collective), the
+ensemble and inverse-problem instances are split over the ranks
+(workloads.partition, no exchange), and rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -176,18 +177,31 @@ def import_package():
     return mod
 
 
-def ensemble(vt, steps: int, n: int = 512, device: int = 0):
+def ensemble(vt, steps: int, n: int = 512, device: int = 0, rank: int = 0, world: int = 1, pg=None):
     """The batched forward ensemble: n seeded vortex problems of uneven size and
     order (workloads.ensemble_instances, seed 1) advanced `steps` RK4 steps as
     one ragged batch (one persistent launch per stage and order group, the step
     in a CUDA graph, grid autotuned), against the same n problems run one at a
     time through the plain solver. Set-up (host precompute, device upload, graph
     capture, tuning) is outside both timed regions; both are host wall-clock
-    around synchronous calls, the device idle at the start of each."""
+    around synchronous calls, the device idle at the start of each.
+
+    With several ranks the instances are split by DOF-stages
+    (workloads.partition, no exchange between ranks); each rank runs its share
+    both ways, and each time is the slowest rank's. Every rank calls this."""
     import torch
     from vortex_transport_b200 import workloads
 
-    inst = workloads.ensemble_instances(n=n, seed=1)
+    inst_all = workloads.ensemble_instances(n=n, seed=1)
+    parts = workloads.partition([workloads.instance_cost(i, steps) for i in inst_all], world)
+    inst = [inst_all[i] for i in parts[rank]]
+
+    def start():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        return time.perf_counter()
+
     t0 = time.perf_counter()
     pbs = workloads.build_problems(inst, threads=os.cpu_count() or 1)
     precompute_s = time.perf_counter() - t0
@@ -195,35 +209,37 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0):
     batch.set_dt([i.dt for i in inst])
     tuned = batch.autotune(trials=2)
     batch.rk4(2)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    t0 = start()
     batch.rk4(steps)
     torch.cuda.synchronize()
-    batched_s = time.perf_counter() - t0
+    batched_s = max_over_ranks(time.perf_counter() - t0, pg)
     groups = batch.groups
     batch.close()
 
-    seq_s = 0.0
+    seq_local = 0.0
     for i, pb in enumerate(pbs):
         s = vt.Solver(pb, device=device)
         s.rk4(inst[i].dt, 2)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s.rk4(inst[i].dt, steps)
-        seq_s += time.perf_counter() - t0
+        seq_local += time.perf_counter() - t0
         s.close()
+    seq_s = max_over_ranks(seq_local, pg)
 
-    dof_stages = 4 * steps * sum(pb.K * pb.Np for pb in pbs)
-    bytes_alg = 4 * steps * sum(pb.K * (128 * pb.Np + 124) for pb in pbs)
+    dof_stages = sum(workloads.instance_cost(i, steps) for i in inst_all)
+    bytes_alg = 4 * steps * sum(2 * i.side * i.side * (128 * (i.p + 1) * (i.p + 2) // 2 + 124) for i in inst_all)
     peak, peak_kind = load_peaks()
-    achieved = bytes_alg / batched_s / 1e9
+    achieved = bytes_alg / batched_s / 1e9 / world
     return {
         "workload": (f"{n} seeded vortex problems (seed 1): side in {{16..128}}, p in {{1,2,3}}, "
                      f"eps~U[0.1,0.5], M~U[0.3,0.7], centre~U[-2,2]^2, perturb~U[0,0.2], io=10, "
                      f"{steps} RK4 steps each"),
         "dt_rule": f"dt = {workloads.ENSEMBLE_CFL} h / ((2p+1)(1 + M^-4)) (0.1 h/(2p+1) is unstable "
                    "in the reference: its Roe dissipation speed is c^4)",
-        "dofs": int(sum(pb.K * pb.Np for pb in pbs)),
+        "dofs": int(workloads.dof_count(inst_all)),
+        "ranks": world,
+        "instances_per_rank": [len(q) for q in parts],
         "groups": [list(g) for g in groups],
         "blocks_per_sm": tuned,
         "batched_solves_per_s": n / batched_s,
@@ -231,7 +247,8 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0):
         "speedup": seq_s / batched_s,
         "batched_dof_stages_per_s": dof_stages / batched_s,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind},
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "note": "per GPU" if world > 1 else "single GPU"},
         "batched_s": batched_s, "sequential_s": seq_s, "precompute_s": precompute_s,
     }
 
@@ -292,37 +309,57 @@ def adjoint(vt, steps: int = 2000, snapshots=None, device: int = 0):
     return out
 
 
-def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0):
+def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0, rank: int = 0, world: int = 1,
+                    pg=None):
     """The batched adjoint inverse problem: n vortices on 64x64 cells (8,192
     triangles), p=2, 300 RK4 steps; seeded true (eps, M, x0, y0) and a
     perturbed guess; per-instance L-BFGS on the host with every loss
     evaluation one batched forward + reverse sweep (every step start kept).
     The time step is the ensemble's stability rule at the lowest Mach number
     the search may try (0.25): 3.65e-5 (1.5e-4 blows up there, as it does in
-    the reference: the Roe dissipation speed is c^4 = M^-4 = 256)."""
+    the reference: the Roe dissipation speed is c^4 = M^-4 = 256).
+
+    With several ranks each solves its share of the vortices (the problems
+    are independent); the solve time is the slowest rank's and the per-vortex
+    results are gathered. Every rank calls this."""
     import numpy as np
+    import torch
     from vortex_transport_b200 import inverse, workloads
 
-    theta = inverse.true_parameters(n, seed=5)
-    guess = inverse.perturbed_guess(theta, seed=6)
+    theta_all = inverse.true_parameters(n, seed=5)
+    guess_all = inverse.perturbed_guess(theta_all, seed=6)
+    mine = workloads.partition([1.0] * n, world)[rank]
+    theta, guess = theta_all[mine], guess_all[mine]
     dt = workloads.stable_dt(64, 2, float(inverse.LOWER[1]))
     t0 = time.perf_counter()
     inv = inverse.BatchedInverse(theta, side=64, p=2, steps=300, dt=dt, device=device)
-    setup_s = time.perf_counter() - t0
+    setup_s = max_over_ranks(time.perf_counter() - t0, pg)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
     t0 = time.perf_counter()
     x, f, done = inv.solve(guess, iterations=iterations)
-    solve_s = time.perf_counter() - t0
-    err0 = np.abs(guess - theta)
-    err = np.abs(x - theta)
+    solve_s = max_over_ranks(time.perf_counter() - t0, pg)
+    evaluations = int(max_over_ranks(float(inv.evaluations), pg))
+    local = {"err0": np.abs(guess - theta).max(axis=1), "err": np.abs(x - theta).max(axis=1), "done": done,
+             "ratio": f / np.maximum(inv.loss_and_grad(guess)[0], 1e-300)}
+    if pg:
+        got = [None] * world
+        pg.all_gather_object(got, local)
+    else:
+        got = [local]
+    err0, err, done_all, ratio = (np.concatenate([g[k] for g in got]) for k in ("err0", "err", "done", "ratio"))
     out = {"workload": f"{n} vortices, 64x64 cells (8,192 triangles) each, p=2, io=10, 300 RK4 steps at "
                        f"dt={dt:.4g}; true eps~U[0.15,0.45], M~U[0.3,0.6], centre~U[-1.5,1.5]^2 (seed 5); "
                        "guess eps/M +-0.05, centre +-0.3 (seed 6)",
-           "iterations_max": iterations, "accepted_steps_median": float(np.median(done)),
-           "evaluations": inv.evaluations, "solve_s": solve_s, "s_per_evaluation": solve_s / inv.evaluations,
+           "ranks": world, "iterations_max": iterations, "accepted_steps_median": float(np.median(done_all)),
+           "evaluations": evaluations, "solve_s": solve_s, "s_per_evaluation": solve_s / evaluations,
+           "iterations_per_s": float(np.median(done_all)) / solve_s,
+           "instance_iterations_per_s": float(np.sum(done_all)) / solve_s,
            "setup_s": setup_s, "max_param_error_initial": float(err0.max()),
            "max_param_error_final": float(err.max()),
-           "median_param_error_final": float(np.median(err.max(axis=1))),
-           "loss_reduction_worst": float((f / np.maximum(inv.loss_and_grad(guess)[0], 1e-300)).max()),
+           "median_param_error_final": float(np.median(err)),
+           "loss_reduction_worst": float(ratio.max()),
            "checkpoints": inv.batch.adjoint_info()}
     inv.close()
     return out
@@ -444,6 +481,11 @@ def b200_arm(args):
     e2e_value = world * dof_stages_per_step * e2e_steps / (e2e_ms * 1e-3) if e2e_steps else None
     state_bytes = K_el * NP * 4 * 8
 
+    # independent instances split over the ranks (all ranks take part)
+    ens = (ensemble(vt, args.ensemble_steps, device=local, rank=rank, world=world, pg=pg)
+           if args.ensemble_steps > 0 else None)
+    inv = (inverse_problem(vt, args.inverse_iters, device=local, rank=rank, world=world, pg=pg)
+           if args.inverse_iters > 0 else None)
     if pg:
         pg.barrier()
     if rank == 0:
@@ -453,9 +495,7 @@ def b200_arm(args):
         achieved = bytes_per_launch / avg_launch_s / 1e9
         traffic = profile_traffic()
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
-        ens = ensemble(vt, args.ensemble_steps, device=local) if world == 1 and args.ensemble_steps > 0 else None
         adj = adjoint(vt, args.adjoint_steps, device=local) if world == 1 and args.adjoint_steps > 0 else None
-        inv = inverse_problem(vt, args.inverse_iters, device=local) if world == 1 and args.inverse_iters > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,

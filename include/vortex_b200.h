@@ -157,7 +157,9 @@ void vt_destroy(vt_ctx* ctx);
  * NULL) are generated per element on the GPU; only the reference-space tables
  * are built on the host. The mesh perturbation uses CUDA's sin/cos/pow, so
  * perturbed vertices agree with vt_problem_create's (glibc) to rounding; the
- * connectivity is identical. */
+ * connectivity is identical. num_element_in_y must be at least 2: with one
+ * row the reference's vertical neighbour index is negative (VT_ERR_INVALID,
+ * as vt_create and vt_batch_create return for such a mesh). */
 vt_ctx* vt_create_structured(const vt_params* prm, const vt_vortex* ic, int device, int* status);
 
 /* State transfer with host arrays in the reference layout (U: K x Np x 4). */
@@ -307,6 +309,11 @@ int vt_adjoint_forward(vt_ctx* ctx, double dt, int nsteps, int nsnapshots);
  * dJ/dU(0), recomputing the steps between checkpoints. Leaves the state and
  * the time alone, and may be called again with another dJ/dU(T). */
 int vt_adjoint_backward(vt_ctx* ctx, const double* dJdU_T, double* dJdU_0, int device_pointers);
+/* Both sweeps in one call, host arrays (K x Np x 4), for a cotangent dJ/dU(T)
+ * known before the run (a linear functional of U(T)); a loss that depends on
+ * U(T) needs the two calls above, with U(T) read in between. The one-call
+ * adjoint entry of the drop-in interface. */
+int vt_adjoint_rk4(vt_ctx* ctx, double dt, int nsteps, int nsnapshots, const double* dJdU_T, double* dJdU_0);
 /* Schedule of the last vt_adjoint_forward. */
 int vt_adjoint_info(const vt_ctx* ctx, vt_checkpoint_info* out);
 

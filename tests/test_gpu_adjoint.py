@@ -159,6 +159,9 @@ def test_tangent_adjoint_dot_product_and_checkpoints(vt, p, io):
     np.testing.assert_array_equal(s.adjoint_backward(lT), lams[0])  # replays the forward sweep
     np.testing.assert_array_equal(s.download(), UT)  # the reverse sweep leaves U(T)
     assert rel(np.sum(lT * dT), np.sum(lams[0] * d0)) < DOT_RTOL
+    s.upload(U0)
+    np.testing.assert_array_equal(s.adjoint_rk4(dt, n, 5, lT), lams[0])  # the one-call entry
+    np.testing.assert_array_equal(s.download(), UT)
 
 
 @pytest.mark.parametrize("p,io", [(3, 10), (2, 6), (1, 4)])

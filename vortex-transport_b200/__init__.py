@@ -181,6 +181,8 @@ _SIGNATURES = {
     "vt_problem_exact_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp]),
     "vt_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
     "vt_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "vt_adjoint_rk4": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p]),
     "vt_adjoint_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "vt_rhs_jvp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_int]),
@@ -605,6 +607,18 @@ class Solver:
         """dJ/dU(0) from dJ/dU(T), for the last adjoint_forward."""
         ins, outp, out, dev, _keep = self._state_args(dJdU_T)
         self._step_status(lib().vt_adjoint_backward(self._h, ins[0], outp, dev))
+        return out
+
+    def adjoint_rk4(self, dt: float, nsteps: int, nsnapshots: int, dJdU_T: np.ndarray) -> np.ndarray:
+        """Both sweeps in one call (vt_adjoint_rk4) for a cotangent known before
+        the run; host arrays K x Np x 4. Leaves U(T) in the solver."""
+        lam = np.ascontiguousarray(dJdU_T, dtype=np.float64)
+        if lam.shape != (self.K, self.Np, 4):
+            raise ValueError(f"dJdU_T must have shape {(self.K, self.Np, 4)}")
+        out = np.empty_like(lam)
+        self._step_status(lib().vt_adjoint_rk4(self._h, float(dt), int(nsteps), int(nsnapshots),
+                                               lam.ctypes.data_as(ctypes.c_void_p),
+                                               out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
     def adjoint_info(self) -> dict:

@@ -519,6 +519,12 @@ int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int dev
   return vt::finish(c, 0, 0.0);
 }
 
+int vt_adjoint_rk4(vt_ctx* c, double dt, int nsteps, int nsnapshots, const double* dJdU_T, double* dJdU_0) {
+  if (!c || !dJdU_T || !dJdU_0) return fail(VT_ERR_INVALID, "vt_adjoint_rk4: null argument");
+  const int st = vt_adjoint_forward(c, dt, nsteps, nsnapshots);
+  return st ? st : vt_adjoint_backward(c, dJdU_T, dJdU_0, 0);
+}
+
 int vt_adjoint_info(const vt_ctx* c, vt_checkpoint_info* out) {
   if (!c || !out) return fail(VT_ERR_INVALID, "vt_adjoint_info: null argument");
   if (!c->adj || !c->adj->have_forward) return fail(VT_ERR_INVALID, "vt_adjoint_info: no forward sweep");

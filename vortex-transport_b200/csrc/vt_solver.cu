@@ -585,6 +585,14 @@ vt_ctx* vt_create_structured(const vt_params* prm, const vt_vortex* ic_in, int d
     set(fail(VT_ERR_INVALID, "vt_create_structured: num_element_in_x/y out of range"));
     return nullptr;
   }
+  // With one row of cells the reference's periodic vertical-neighbour formula
+  // (Meshgeneration.cpp:94-117) gives every even element a negative index, a
+  // mesh vt_create rejects as well; the device set-up never builds one.
+  if (ny < 2) {
+    set(fail(VT_ERR_INVALID, "vt_create_structured: num_element_in_y must be at least 2 (the reference's "
+                             "vertical neighbour of a single row is out of range)"));
+    return nullptr;
+  }
   const vt_vortex ic = ic_in ? *ic_in : vt::default_vortex();
   // reference-space tables (host, a few KB)
   const int p = prm->p, Np = vt::np_of(p);

@@ -75,3 +75,25 @@ def build_problems(instances, threads: int = 16) -> list[Problem]:
 
 def dof_count(instances) -> int:
     return sum(2 * i.side * i.side * (i.p + 1) * (i.p + 2) // 2 for i in instances)
+
+
+def partition(costs, world: int) -> list[list[int]]:
+    """Independent instances over `world` ranks with no exchange between them:
+    longest first, each to the least-loaded rank (ties to the lower rank), so
+    every rank's share is within one instance's cost of the mean. Returns the
+    instance indices of each rank, ascending; deterministic, so every rank
+    computes the same split without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda j: (-costs[j], j)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def instance_cost(inst: Instance, steps: int = 1) -> int:
+    """DOF-stages of `steps` RK4 steps of one instance (the work a rank takes on)."""
+    return 4 * steps * dof_count([inst])
