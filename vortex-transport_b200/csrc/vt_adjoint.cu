@@ -6,8 +6,9 @@
 // of vt_checkpoint.h says, or, when the snapshot budget holds four states per
 // step, writes every step's start and stage states to their own buffers.
 // Reverse sweep, per step i = n-1 .. 0: (binomial plan) rerun step i from its
-// checkpoint keeping the stage states U1, U2, U3; then four reverse stages (a
-// face phase + adjoint_element_kernel each) turn the adjoint of U_{i+1} into
+// checkpoint keeping the stage states U1, U2, U3; then four reverse stages
+// (adjoint_tile_kernel each on meshes whose faces take the edge-once form,
+// else a face phase + adjoint_element_kernel) turn the adjoint of U_{i+1} into
 // the adjoint of U_i:
 //   a4 = dt/6 lam                 g4 = R'(U3)^T a4
 //   a3 = dt/3 lam + dt   g4       g3 = R'(U2)^T a3
@@ -25,6 +26,7 @@
 
 #include "../../include/vortex_b200.h"
 #include "vt_adjoint_kernels.cuh"
+#include "vt_adjoint_tile.cuh"
 #include "vt_checkpoint.h"
 #include "vt_common.h"
 #include "vt_ctx.h"
@@ -33,14 +35,17 @@ namespace vt {
 namespace {
 
 using FaceFn = cudaError_t (*)(const AdjArgs&, const double*, cudaStream_t);
+using TileFn = cudaError_t (*)(const AdjArgs&, const double*, int, cudaStream_t);
+using TileConfigFn = cudaError_t (*)(int*);
 using JvpFn = cudaError_t (*)(const double2*, const double2*, double2*, const double2*, const int4*, long long,
                               int, const double*, cudaStream_t);
 
 struct AdjKernels {
   FaceFn face = nullptr;
-  FaceFn edge = nullptr;
   FaceFn element = nullptr;
   JvpFn jvp = nullptr;
+  TileFn tile = nullptr;
+  TileConfigFn tile_config = nullptr;
 };
 
 template <int P, int NFQ>
@@ -53,21 +58,31 @@ cudaError_t launch_face(const AdjArgs& a, const double* ops, cudaStream_t st) {
 }
 
 template <int P, int NFQ>
-cudaError_t launch_edge(const AdjArgs& a, const double* ops, cudaStream_t st) {
-  StageOps<P, NFQ> o;
-  std::memcpy(&o, ops, sizeof(o));
-  const dim3 grid((a.nowners + kAdjRun - 1) / kAdjRun, 3), block(kAdjRun, NFQ);
-  adjoint_edge_kernel<P, NFQ><<<grid, block, 0, st>>>(a, o);
-  return cudaGetLastError();
-}
-
-template <int P, int NFQ>
 cudaError_t launch_element(const AdjArgs& a, const double* ops, cudaStream_t st) {
   StageOps<P, NFQ> o;
   std::memcpy(&o, ops, sizeof(o));
   const dim3 grid((a.K + kAdjRun - 1) / kAdjRun), block(kAdjRun, np_of_p(P));
   adjoint_element_kernel<P, NFQ><<<grid, block, 0, st>>>(a, o);
   return cudaGetLastError();
+}
+
+// One reverse stage as one persistent launch over the stage kernel's tiles.
+template <int P, int NFQ>
+cudaError_t launch_tile(const AdjArgs& a, const double* ops, int max_blocks, cudaStream_t st) {
+  StageOps<P, NFQ> o;
+  std::memcpy(&o, ops, sizeof(o));
+  const int grid = a.ntiles < max_blocks ? a.ntiles : max_blocks;
+  adjoint_tile_kernel<P, NFQ><<<grid, 4 * kTileElems, AdjTileLayout<P, NFQ>::kBytes, st>>>(a, o);
+  return cudaGetLastError();
+}
+
+template <int P, int NFQ>
+cudaError_t configure_tile(int* blocks_per_sm) {
+  constexpr int bytes = AdjTileLayout<P, NFQ>::kBytes;
+  cudaError_t e = cudaFuncSetAttribute(adjoint_tile_kernel<P, NFQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint_tile_kernel<P, NFQ>, 4 * kTileElems,
+                                                       bytes);
 }
 
 template <int P, int NFQ>
@@ -81,7 +96,8 @@ cudaError_t launch_jvp(const double2* U, const double2* V, double2* dR, const do
 
 template <int P, int NFQ>
 AdjKernels kernels_of() {
-  return AdjKernels{launch_face<P, NFQ>, launch_edge<P, NFQ>, launch_element<P, NFQ>, launch_jvp<P, NFQ>};
+  return AdjKernels{launch_face<P, NFQ>, launch_element<P, NFQ>, launch_jvp<P, NFQ>, launch_tile<P, NFQ>,
+                    configure_tile<P, NFQ>};
 }
 
 template <int P>
@@ -134,11 +150,10 @@ struct AdjointState {
   double2 *work = nullptr, *s1 = nullptr, *s2 = nullptr, *s3 = nullptr;
   double2 *lam = nullptr, *acc = nullptr, *a0 = nullptr, *a1 = nullptr;
   double2 *bp = nullptr, *bm = nullptr;  // face adjoints
-  // edge-once face phase: owner elements (null when the mesh does not 2-colour)
-  int* owners = nullptr;
-  int* owner_nb = nullptr;  // [3][nowners]
-  unsigned char* is_owner = nullptr;
-  int nowners = 0;
+  // fused reverse stage (adjoint_tile_kernel): persistent grid size, 0 when
+  // the edge-once form does not apply (the element adjacency does not
+  // 2-colour) or the kernel cannot be resident
+  int tile_blocks = 0;
   double2* slots = nullptr;
   long long nslots = 0;
   // last forward sweep
@@ -177,8 +192,10 @@ int setup(vt_ctx* c) {
   s->bp = s->bufs + 8 * s->state_elems;
   s->bm = s->bp + face_elems;
   c->adj = s;
-  // Owners for the edge-once face phase: a 2-colouring of the element
-  // adjacency (breadth first); colour 0 owns every edge it touches.
+  // The edge-once form needs every edge to join elements whose sides face each
+  // other with opposite normals; a 2-colouring of the element adjacency
+  // (breadth first) tells such meshes (the reference's type-0 / type-1
+  // triangles) from ones with self-neighbours or odd cycles.
   std::vector<int4> nb(static_cast<size_t>(c->K));
   e = cudaMemcpy(nb.data(), c->nbr, sizeof(int4) * nb.size(), cudaMemcpyDeviceToHost);
   if (e) return fail(VT_ERR_CUDA, cuda_msg("adjoint: neighbours", e));
@@ -203,28 +220,12 @@ int setup(vt_ctx* c) {
     }
   }
   if (ok) {
-    std::vector<int> owners;
-    std::vector<unsigned char> flag(nb.size());
-    for (int x = 0; x < c->K; ++x) {
-      flag[x] = col[x] == 0;
-      if (flag[x]) owners.push_back(x);
-    }
-    const size_t no = owners.size();
-    s->nowners = static_cast<int>(no);
-    // owners, then their neighbours per side, then the owner flags
-    for (int sd = 0; sd < 3; ++sd)
-      for (size_t i = 0; i < no; ++i) {
-        const int4 b = nb[owners[i]];
-        owners.push_back(sd == 0 ? b.x : (sd == 1 ? b.y : b.z));
-      }
-    e = cudaMalloc(reinterpret_cast<void**>(&s->owners), sizeof(int) * owners.size() + flag.size());
-    if (!e) {
-      s->owner_nb = s->owners + no;
-      s->is_owner = reinterpret_cast<unsigned char*>(s->owners + owners.size());
-      e = cudaMemcpy(s->owners, owners.data(), sizeof(int) * owners.size(), cudaMemcpyHostToDevice);
-    }
-    if (!e) e = cudaMemcpy(s->is_owner, flag.data(), flag.size(), cudaMemcpyHostToDevice);
-    if (e) return fail(VT_ERR_CUDA, cuda_msg("adjoint: owners", e));
+    // the fused reverse stage runs on the stage kernel's tiles
+    int per_sm = 0, sms = 0;
+    if (c->tiles && c->ntiles > 0 && !s->k.tile_config(&per_sm) &&
+        !cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) && per_sm > 0)
+      s->tile_blocks = sms * per_sm;
+    cudaGetLastError();
   }
   return VT_OK;
 }
@@ -294,21 +295,27 @@ AdjArgs adj_args(vt_ctx* c) {
   a.bp = c->adj->bp;
   a.bm = c->adj->bm;
   a.elem_dt = c->elem_dt;
-  a.owners = c->adj->owners;
-  a.owner_nb = c->adj->owner_nb;
-  a.is_owner = c->adj->is_owner;
-  a.nowners = c->adj->nowners;
   a.geo = c->geo;
   a.nbr = c->nbr;
+  a.tiles = c->tiles;
+  a.tile_items = c->tile_items;
+  a.tile_count = c->tile_count;
+  a.ntiles = c->ntiles;
+  a.err = c->err;
   a.Kpad = c->Kpad;
   a.K = c->K;
   a.sa = 1.0;
   return a;
 }
 
+// One reverse stage: the fused tile kernel where the face phase may take the
+// edge-once form, else the two-sided face phase and the element kernel (exact
+// on any mesh whose sides pair up).
 cudaError_t reverse_stage(vt_ctx* c, const AdjArgs& a) {
-  cudaError_t e = a.is_owner ? c->adj->k.edge(a, c->ops.data(), c->stream) : c->adj->k.face(a, c->ops.data(), c->stream);
-  return e ? e : c->adj->k.element(a, c->ops.data(), c->stream);
+  AdjointState* s = c->adj;
+  if (s->tile_blocks > 0) return s->k.tile(a, c->ops.data(), s->tile_blocks, c->stream);
+  const cudaError_t e = s->k.face(a, c->ops.data(), c->stream);
+  return e ? e : s->k.element(a, c->ops.data(), c->stream);
 }
 
 // lam <- adjoint of U_i given lam = adjoint of U_{i+1}; X = U_i, stage states S1..S3.
@@ -414,7 +421,6 @@ void adjoint_release(vt_ctx* c) {
   if (!c || !c->adj) return;
   c->adj->fwd_graph.reset();
   c->adj->bwd_graph.reset();
-  if (c->adj->owners) cudaFree(c->adj->owners);
   if (c->adj->slots) cudaFree(c->adj->slots);
   if (c->adj->bufs) cudaFree(c->adj->bufs);
   delete c->adj;
@@ -556,7 +562,8 @@ int vt_rhs_vjp(vt_ctx* c, const double* U, const double* W, double* G, int devic
   if (st) return st;
   vt::AdjointState* s = c->adj;
   s->fresh = false;
-  cudaError_t e = vt::load_aos(c, U, device_pointers, s->s1);
+  cudaError_t e = vt::reset_error_words(c);
+  if (!e) e = vt::load_aos(c, U, device_pointers, s->s1);
   if (!e) e = vt::load_aos(c, W, device_pointers, s->s2);
   if (!e) {
     vt::AdjArgs a = vt::adj_args(c);
@@ -564,8 +571,8 @@ int vt_rhs_vjp(vt_ctx* c, const double* U, const double* W, double* G, int devic
     e = vt::reverse_stage(c, a);
   }
   if (!e) e = vt::store_aos(c, s->s3, G, device_pointers);
-  if (!e) e = cudaStreamSynchronize(c->stream);
-  return e ? fail(VT_ERR_CUDA, vt::cuda_msg("rhs vjp", e)) : VT_OK;
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("rhs vjp", e));
+  return vt::finish(c, 0, 0.0);
 }
 
 int vt_tangent_rk4(vt_ctx* c, double dt, int nsteps, const double* dU_0, double* dU_T, int device_pointers) {

@@ -18,12 +18,8 @@
 //                           faces (tm, bm of the neighbour across side s, whose
 //                           side s faces e), then the reverse RK4 combine.
 //
-// On a mesh whose elements 2-colour into owners and non-owners (every edge joins
-// one of each, as the reference's type-0/type-1 triangles do), the face phase
-// is adjoint_edge_kernel instead: the Roe flux is antisymmetric,
-// F(u-, u+, -n) = -F(u+, u-, n), and the neighbour's face point NFQ-1-q is the
-// owner's point q, so one transposed Roe Jacobian per edge point, applied to
-// bF_owner(q) - bF_neighbour(NFQ-1-q), serves both sides.
+// On meshes whose faces take the edge-once form the whole reverse stage is
+// one launch instead, adjoint_tile_kernel (vt_adjoint_tile.cuh).
 //
 // Both read the state through the SoA-of-double2 layout of the stage kernel,
 // so a warp's 32 consecutive elements are contiguous 512-byte rows. The
@@ -47,17 +43,16 @@ struct AdjArgs {
   double2* bm;            // face adjoints, neighbour trace
   const double2* geo;
   const int4* nbr;
-  // Edge-once form (null is_owner: every element evaluates its own faces): the
-  // elements split into owners and non-owners with every edge joining one of
-  // each; an owner evaluates each of its edges once for both sides.
-  const int* owners;                // owner elements, nowners of them
-  const int* owner_nb;              // [3][nowners]: each owner's neighbour across side s
-  const unsigned char* is_owner;    // K flags, or null
-  int nowners;
   // Per-element time steps (a batch group with uneven steps), or null: then
   // sa (when sa_dt is set), cl and cg are fractions of the element's step.
   const double* elem_dt;
   int sa_dt;
+  // The stage kernel's tile schedule (adjoint_tile_kernel) and error words.
+  const int4* tiles;
+  const int* tile_items;
+  const int* tile_count;
+  int ntiles;
+  unsigned long long* err;
   long long Kpad;
   int K;
   double sa, lam_coef, cl, cg;
@@ -108,100 +103,6 @@ __global__ void __launch_bounds__(kAdjRun * NFQ)
 #pragma unroll
   for (int c = 0; c < 4; ++c) bf[c] *= sc;
   const double2 n = __ldg(a.geo + (2 + s) * KP + e);
-  double bu[4] = {0.0, 0.0, 0.0, 0.0}, bv[4] = {0.0, 0.0, 0.0, 0.0};
-  roe_flux_vjp(up, um, n.x, n.y, bf, bu, bv);
-  const long long r0 = static_cast<long long>(2 * w) * KP + e;
-  a.bp[r0] = make_double2(bu[0], bu[1]);
-  a.bp[r0 + KP] = make_double2(bu[2], bu[3]);
-  a.bm[r0] = make_double2(bv[0], bv[1]);
-  a.bm[r0 + KP] = make_double2(bv[2], bv[3]);
-}
-
-// Block: 32 owners (lanes) x NFQ face points (warps) of one side s. The
-// operands every face point of an edge shares (both elements' adjoints, the
-// side's node states of both) are staged once per block in shared memory.
-template <int P, int NFQ>
-__global__ void __launch_bounds__(kAdjRun * NFQ, NFQ <= 6 ? 4 : 2)
-    adjoint_edge_kernel(const AdjArgs a, const StageOps<P, NFQ> o) {
-  constexpr int NP = np_of_p(P), NE = P + 1;
-  constexpr int RA = 2 * NP, RU = 2 * NE, RG = 2 * RA + 2 * RU, ROWS = RG + 5;
-  // a(e), a(nb), U(e) side nodes, U(nb) side nodes, then geometry: rows 5-6 of
-  // e and of nb (side lengths / det J) and the normal of side s of e
-  __shared__ double2 sh[ROWS][kAdjRun];
-  __shared__ int sE[kAdjRun], sN[kAdjRun];
-  const int s = blockIdx.y, q = threadIdx.y;  // uniform per block / warp
-  const int lane = threadIdx.x, tid = q * kAdjRun + lane;
-  const int i0 = blockIdx.x * kAdjRun;
-  const long long KP = a.Kpad;
-  if (tid < kAdjRun) {
-    const bool ok = i0 + tid < a.nowners;
-    sE[tid] = ok ? __ldg(a.owners + i0 + tid) : -1;
-    sN[tid] = ok ? __ldg(a.owner_nb + static_cast<long long>(s) * a.nowners + i0 + tid) : -1;
-  }
-  __syncthreads();
-  for (int l = tid; l < ROWS * kAdjRun; l += kAdjRun * NFQ) {
-    const int row = l / kAdjRun, ln = l % kAdjRun;
-    const int e = sE[ln], nb = sN[ln];
-    if (e < 0) continue;
-    double2 v;
-    if (row < RA) {
-      v = __ldg(a.a + row * KP + e);
-    } else if (row < 2 * RA) {
-      v = __ldg(a.a + (row - RA) * KP + nb);
-    } else if (row < RG) {
-      const int r = row < 2 * RA + RU ? row - 2 * RA : row - 2 * RA - RU;
-      const int node = edge_node(P, s, r >> 1);
-      v = __ldg(a.U + (2 * node + (r & 1)) * KP + (row < 2 * RA + RU ? e : nb));
-    } else {
-      const int g = row - RG;  // 0,1: rows 5,6 of e; 2,3: rows 5,6 of nb; 4: normal of side s
-      v = g < 4 ? __ldg(a.geo + (5 + (g & 1)) * KP + (g < 2 ? e : nb)) : __ldg(a.geo + (2 + s) * KP + e);
-    }
-    sh[row][ln] = v;
-  }
-  __syncthreads();
-  const int e = sE[lane];
-  if (e < 0) return;
-  const int qm = NFQ - 1 - q, w = s * NFQ + q;
-  double up[4] = {0.0, 0.0, 0.0, 0.0}, um[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-  for (int k = 0; k < NE; ++k) {
-    const double cp = o.tp[s][q][k], cm = o.tm[s][q][k];
-    const double2 x0 = sh[2 * RA + 2 * k][lane], x1 = sh[2 * RA + 2 * k + 1][lane];
-    const double2 y0 = sh[2 * RA + RU + 2 * k][lane], y1 = sh[2 * RA + RU + 2 * k + 1][lane];
-    up[0] = fma(cp, x0.x, up[0]);
-    up[1] = fma(cp, x0.y, up[1]);
-    up[2] = fma(cp, x1.x, up[2]);
-    up[3] = fma(cp, x1.y, up[3]);
-    um[0] = fma(cm, y0.x, um[0]);
-    um[1] = fma(cm, y0.y, um[1]);
-    um[2] = fma(cm, y1.x, um[2]);
-    um[3] = fma(cm, y1.y, um[3]);
-  }
-  // owner side: R_e -= ls_e lift[s][.][q] F(q); neighbour side: R_nb += ls_nb lift[s][.][qm] F(q)
-  double be[4] = {0.0, 0.0, 0.0, 0.0}, bn[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-  for (int j = 0; j < NP; ++j) {
-    const double l = o.lift[s][j][q], lm = o.lift[s][j][qm];
-    const double2 a0 = sh[2 * j][lane], a1 = sh[2 * j + 1][lane];
-    const double2 c0 = sh[RA + 2 * j][lane], c1 = sh[RA + 2 * j + 1][lane];
-    be[0] = fma(l, a0.x, be[0]);
-    be[1] = fma(l, a0.y, be[1]);
-    be[2] = fma(l, a1.x, be[2]);
-    be[3] = fma(l, a1.y, be[3]);
-    bn[0] = fma(lm, c0.x, bn[0]);
-    bn[1] = fma(lm, c0.y, bn[1]);
-    bn[2] = fma(lm, c1.x, bn[2]);
-    bn[3] = fma(lm, c1.y, bn[3]);
-  }
-  const double2 lea = sh[RG][lane], leb = sh[RG + 1][lane];
-  const double2 lna = sh[RG + 2][lane], lnb = sh[RG + 3][lane];
-  const double sa = (a.elem_dt && a.sa_dt) ? a.sa * __ldg(a.elem_dt + e) : a.sa;  // nb: same instance
-  const double se = -(s == 0 ? lea.x : (s == 1 ? lea.y : leb.x)) * sa;
-  const double sn = (s == 0 ? lna.x : (s == 1 ? lna.y : lnb.x)) * sa;
-  double bf[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) bf[c] = fma(se, be[c], sn * bn[c]);
-  const double2 n = sh[RG + 4][lane];
   double bu[4] = {0.0, 0.0, 0.0, 0.0}, bv[4] = {0.0, 0.0, 0.0, 0.0};
   roe_flux_vjp(up, um, n.x, n.y, bf, bu, bv);
   const long long r0 = static_cast<long long>(2 * w) * KP + e;
@@ -268,10 +169,7 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P), 3)
     const double sv[4] = {u0.x, u0.y, u1.x, u1.y};
     contravariant_vjp(sv, j0.x, j0.y, j1.x, j1.y, bx, by, g);
   }
-  // two-sided faces: own bp (tp) and the neighbour's bm (tm); edge-once: an
-  // owner takes bp of its evaluation, a non-owner bm of its neighbour's
-  const bool use_p = !a.is_owner || a.is_owner[e];
-  const bool use_m = !a.is_owner || !a.is_owner[e];
+  // two-sided faces: own bp (tp) and the neighbour's bm (tm)
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
     const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
@@ -281,22 +179,17 @@ __global__ void __launch_bounds__(kAdjRun * np_of_p(P), 3)
 #pragma unroll
       for (int q = 0; q < NFQ; ++q) {
         const long long r0 = static_cast<long long>(2 * (s * NFQ + q)) * KP;
-        if (use_p) {
-          const double cp = o.tp[s][q][k];
-          const double2 p0 = __ldg(a.bp + r0 + e), p1 = __ldg(a.bp + r0 + KP + e);
-          g[0] = fma(cp, p0.x, g[0]);
-          g[1] = fma(cp, p0.y, g[1]);
-          g[2] = fma(cp, p1.x, g[2]);
-          g[3] = fma(cp, p1.y, g[3]);
-        }
-        if (use_m) {
-          const double cm = o.tm[s][q][k];
-          const double2 m0 = __ldg(a.bm + r0 + nb), m1 = __ldg(a.bm + r0 + KP + nb);
-          g[0] = fma(cm, m0.x, g[0]);
-          g[1] = fma(cm, m0.y, g[1]);
-          g[2] = fma(cm, m1.x, g[2]);
-          g[3] = fma(cm, m1.y, g[3]);
-        }
+        const double cp = o.tp[s][q][k], cm = o.tm[s][q][k];
+        const double2 p0 = __ldg(a.bp + r0 + e), p1 = __ldg(a.bp + r0 + KP + e);
+        g[0] = fma(cp, p0.x, g[0]);
+        g[1] = fma(cp, p0.y, g[1]);
+        g[2] = fma(cp, p1.x, g[2]);
+        g[3] = fma(cp, p1.y, g[3]);
+        const double2 m0 = __ldg(a.bm + r0 + nb), m1 = __ldg(a.bm + r0 + KP + nb);
+        g[0] = fma(cm, m0.x, g[0]);
+        g[1] = fma(cm, m0.y, g[1]);
+        g[2] = fma(cm, m1.x, g[2]);
+        g[3] = fma(cm, m1.y, g[3]);
       }
     }
   }

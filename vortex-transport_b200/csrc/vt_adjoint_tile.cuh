@@ -1,0 +1,414 @@
+// One reverse RK stage fused into one kernel on the stage kernel's tiles.
+//
+// The transpose of the stage right-hand side R at the stage state U applied to
+// the stage adjoint a (times sa), g = R'(U)^T (sa a), followed by the reverse
+// RK4 combine of adjoint_element_kernel, for meshes on which the face phase
+// may take the edge-once form (a face's flux is evaluated once for both
+// sides: F(u-, u+, -n) = -F(u+, u-, n)). A persistent block walks the forward
+// stage kernel's tiles (64 elements, two runs, vt_schedule.cuh) and keeps every
+// intermediate in shared memory, so nothing but the state, the adjoints and
+// the geometry crosses HBM:
+//
+//   1. load   the tile's stage-state rows by TMA bulk copies (issued during the
+//             previous tile), the side-0 neighbours' side nodes, the face list;
+//   2. lift^T thread (element, component): the lifted face adjoint
+//             bF(s, q) = -(len_s/detJ) sa sum_i LIFT_s[i][q] a_i at every face
+//             point (the transpose of the lift and of the folded mass inverse);
+//   3. faces  one work item per face point of the tile's face list. A face
+//             between two tile elements is taken once: the transposed Roe
+//             Jacobian at (U+, U-) applied to bF_e(q) - bF_nb(nfq-1-q) gives
+//             the adjoints of both traces, each written over its element's bF
+//             slot. A face leaving the tile is taken by each side, with the
+//             neighbour's bF recomputed from its stage adjoint, and gives the
+//             own trace's adjoint only (the neighbour's tile takes the other);
+//   4. traces^T  thread (element, component): the trace adjoints onto the
+//             side nodes (transposed trace weights) into Np accumulators; then
+//             the transposed volume operator sa sum_i D[d][i][j] a_i per node;
+//   5. flux^T the transposed nodal flux Jacobian of every node (its state in
+//             shared memory), once; the state tile is then free and the next
+//             tile's copies are issued;
+//   6. combine acc_out = acc_in + lam_coef lam + g, a_out = cl lam + cg g.
+//
+// Every wait on the mbarrier is bounded; a wait that gives up sets bit 1 of
+// err[3] and the block stops taking tiles.
+#pragma once
+
+#include "vt_adjoint.cuh"
+#include "vt_adjoint_kernels.cuh"
+#include "vt_tile.cuh"
+
+namespace vt {
+
+// The stage kernel's shared-memory layout plus the two operator tables the
+// face phase indexes at run time (side and face point differ across a warp).
+template <int P, int NFQ>
+struct AdjTileLayout {
+  using Base = TileLayout<P, NFQ>;
+  static constexpr int NP = Base::NP;
+  static constexpr int NE = Base::NE;
+  static constexpr int kTP = align16(Base::kBytes);            // double [3][NFQ][NE] own trace weights
+  static constexpr int kLF = align16(kTP + 3 * NFQ * NE * 8);  // double [3][NP][NFQ] LIFT
+  static constexpr int kBytes = align16(kLF + 3 * NP * NFQ * 8);
+};
+
+// component c of node i of an SoA double2 state, element e
+__device__ __forceinline__ long long comp_index(long long KP, int i, int c, int e) {
+  return ((2 * i + (c >> 1)) * KP + e) * 2 + (c & 1);
+}
+
+// Two 256-thread blocks per SM: the transposed Roe Jacobian needs about 128
+// registers per thread; capped at 80 (three blocks) it spills 416 bytes and the
+// reverse stage runs 18% slower.
+template <int P, int NFQ>
+__global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const AdjArgs a,
+                                                                          const StageOps<P, NFQ> ops) {
+  using B = TileLayout<P, NFQ>;
+  using L = AdjTileLayout<P, NFQ>;
+  constexpr int E = B::E;
+  constexpr int NP = B::NP;
+  constexpr int NE = B::NE;
+  constexpr int ES = B::ES;
+  constexpr int T = 4 * E;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* S = reinterpret_cast<double2*>(smem + B::kS);
+  double2* H = reinterpret_cast<double2*>(smem + B::kH);
+  double* FB = reinterpret_cast<double*>(smem + B::kFB);
+  double* TM = reinterpret_cast<double*>(smem + B::kTM);
+  int4* NB = reinterpret_cast<int4*>(smem + B::kNB);
+  int* EL = reinterpret_cast<int*>(smem + B::kEL);
+  int* items = reinterpret_cast<int*>(smem + B::kItems);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + B::kBar);
+  int* abort_flag = reinterpret_cast<int*>(smem + B::kBar + 8);
+  double* TP = reinterpret_cast<double*>(smem + L::kTP);
+  double* LF = reinterpret_cast<double*>(smem + L::kLF);
+
+  const int t = threadIdx.x;
+  const int col = t % E, grp = t / E;
+  const int lane = t & 31;
+  const long long KP = a.Kpad;
+  const int G = gridDim.x;
+  const double* Ad = reinterpret_cast<const double*>(a.a);
+
+  {
+    const double* tm = &ops.tm[0][0][0];
+    const double* tp = &ops.tp[0][0][0];
+    const double* lf = &ops.lift[0][0][0];
+    for (int l = t; l < 3 * NFQ * NE; l += T) {
+      TM[l] = tm[l];
+      TP[l] = tp[l];
+    }
+    for (int l = t; l < 3 * NP * NFQ; l += T) LF[l] = lf[l];
+  }
+  if (t == 0) {
+    mbar_init(bar, 1);
+    *abort_flag = 0;
+  }
+  __syncthreads();
+
+  int tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  int4 run = __ldg(a.tiles + tile);
+  int nitems = __ldg(a.tile_count + tile);
+  int my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
+  int4 my_nb = make_int4(0, 0, 0, 0);
+  double2 hreg[2];
+  {
+    const int pos = col % kTileRun;
+    const bool second = col >= kTileRun;
+    const bool valid = pos < (second ? run.w : run.y);
+    if (valid) my_nb = __ldg(a.nbr + (second ? run.z : run.x) + pos);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int r = grp + 4 * k;
+      hreg[k] = (valid && r < 2 * NE) ? __ldg(a.U + r * KP + my_nb.x) : make_double2(1.0, 0.0);
+    }
+  }
+  if (t < 32) issue_tile_copies<NP, ES>(a.U, KP, run, S, bar, lane);
+  unsigned parity = 0;
+
+  for (; tile < a.ntiles; tile += G) {
+    const bool has_next = tile + G < a.ntiles;
+
+    // ---- prefetch into L2: the next tile's state, geometry, neighbour and
+    // adjoint rows; this tile's lam / acc_in rows (read in phase 6) -------------
+    if (t < 64) {
+      if (has_next) {
+        const int4 rr = __ldg(a.tiles + tile + G);
+        const int which = t & 1, r = t >> 1;
+        const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
+        if (len > 0) {
+          const unsigned bytes = static_cast<unsigned>(len) * 16u;
+          if (r < 2 * NP) prefetch_l2(a.U + r * KP + start, bytes);
+          else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
+          else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
+        }
+      }
+    } else if (t < 64 + 8 * NP) {
+      const int l = t - 64, which = l & 1, r = l >> 1;
+      if (r < 2 * NP) {
+        if (has_next) {
+          const int4 rr = __ldg(a.tiles + tile + G);
+          const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
+          if (len > 0) prefetch_l2(a.a + r * KP + start, static_cast<unsigned>(len) * 16u);
+        }
+      } else {
+        const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+        const double2* src = a.lam ? a.lam : a.acc_in;
+        if (len > 0 && src) prefetch_l2(src + (r - 2 * NP) * KP + start, static_cast<unsigned>(len) * 16u);
+      }
+    }
+
+    // ---- 1. load ------------------------------------------------------------------
+    int4 next_run = make_int4(0, 0, 0, 0);
+    if (has_next) next_run = __ldg(a.tiles + tile + G);
+    {
+      const int pos = col % kTileRun;
+      const bool second = col >= kTileRun;
+      const bool valid = pos < (second ? run.w : run.y);
+      if (grp == 0) {
+        NB[col] = my_nb;
+        EL[col] = valid ? (second ? run.z : run.x) + pos : -1;
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int r = grp + 4 * k;
+        if (r < 2 * NE) H[r * ES + col] = hreg[k];
+      }
+      if (t < nitems) items[t] = my_item;
+    }
+    {
+      bool ok = false;
+      for (unsigned n = 0; n < kMaxWaitTries && !ok; ++n) ok = mbar_try_wait(bar, parity);
+      if (!ok) {
+        atomicOr(&a.err[3], 2ull);
+        *abort_flag = 1;
+      }
+    }
+    parity ^= 1u;
+    __syncthreads();
+    if (*abort_flag) break;
+
+    // ---- 2. lifted face adjoints bF[s][c][q][el], thread (element el, component c) ----
+    const int c = grp;  // uniform per warp
+    const int el = col;
+    const int e = EL[el];
+    const bool valid = e >= 0;
+    const double sa = valid && a.elem_dt && a.sa_dt ? a.sa * __ldg(a.elem_dt + e) : a.sa;
+    {
+      double lam[NP];
+      double2 lsa = make_double2(0.0, 0.0), lsb = lsa;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) lam[i] = valid ? __ldg(Ad + comp_index(KP, i, c, e)) : 0.0;
+      if (valid) {
+        lsa = __ldg(a.geo + 5 * KP + e);
+        lsb = __ldg(a.geo + 6 * KP + e);
+      }
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const double sc = -(s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x)) * sa;
+#pragma unroll
+        for (int q = 0; q < NFQ; ++q) {
+          double v = 0.0;
+#pragma unroll
+          for (int i = 0; i < NP; ++i) v = fma(ops.lift[s][i][q], lam[i], v);
+          FB[((s * 4 + c) * NFQ + q) * ES + el] = sc * v;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 3. faces: transposed Roe Jacobian; the trace adjoints overwrite bF ----------
+    for (int w = t; w < nitems * NFQ; w += T) {
+      const int it = items[w / NFQ];
+      const int q = w % NFQ;
+      const int fl = it & 0xff, s = (it >> 8) & 3;
+      const bool mirror = (it >> 10) & 1;
+      const int nl = (it >> 11) & 0xff;
+      const int qm = NFQ - 1 - q;
+      const int fe = EL[fl];
+      const double2 n = __ldg(a.geo + (2 + s) * KP + fe);
+      double up[4] = {0.0, 0.0, 0.0, 0.0}, um[4] = {0.0, 0.0, 0.0, 0.0}, bn[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int k = 0; k < NE; ++k) {
+        const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
+        const double cp = TP[(s * NFQ + q) * NE + k];
+        const double2 x0 = S[(2 * node) * ES + fl], x1 = S[(2 * node + 1) * ES + fl];
+        up[0] = fma(cp, x0.x, up[0]);
+        up[1] = fma(cp, x0.y, up[1]);
+        up[2] = fma(cp, x1.x, up[2]);
+        up[3] = fma(cp, x1.y, up[3]);
+      }
+      if (mirror) {
+        // the partner's own trace at its point nfq-1-q, as the stage kernel reads it
+#pragma unroll
+        for (int k = 0; k < NE; ++k) {
+          const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
+          const double cm = TP[(s * NFQ + qm) * NE + k];
+          const double2 y0 = S[(2 * node) * ES + nl], y1 = S[(2 * node + 1) * ES + nl];
+          um[0] = fma(cm, y0.x, um[0]);
+          um[1] = fma(cm, y0.y, um[1]);
+          um[2] = fma(cm, y1.x, um[2]);
+          um[3] = fma(cm, y1.y, um[3]);
+        }
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) bn[cc] = FB[((s * 4 + cc) * NFQ + qm) * ES + nl];
+      } else {
+        const int4 nb4 = NB[fl];
+        const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
+#pragma unroll
+        for (int k = 0; k < NE; ++k) {
+          const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
+          const double cm = TM[(s * NFQ + q) * NE + k];
+          double2 y0, y1;
+          if (s == 0) {
+            y0 = H[(2 * k) * ES + fl];
+            y1 = H[(2 * k + 1) * ES + fl];
+          } else {
+            y0 = __ldg(a.U + (2 * node) * KP + nb);
+            y1 = __ldg(a.U + (2 * node + 1) * KP + nb);
+          }
+          um[0] = fma(cm, y0.x, um[0]);
+          um[1] = fma(cm, y0.y, um[1]);
+          um[2] = fma(cm, y1.x, um[2]);
+          um[3] = fma(cm, y1.y, um[3]);
+        }
+        // the neighbour's lifted adjoint at its point nfq-1-q, formed as its own tile forms it
+        const double san = a.elem_dt && a.sa_dt ? a.sa * __ldg(a.elem_dt + nb) : a.sa;
+        const double* gn = reinterpret_cast<const double*>(a.geo + (s < 2 ? 5 : 6) * KP + nb);
+        const double sc = -__ldg(gn + (s == 1 ? 1 : 0)) * san;
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          const double l = LF[(s * NP + i) * NFQ + qm];
+          const double2 a0 = __ldg(a.a + (2 * i) * KP + nb), a1 = __ldg(a.a + (2 * i + 1) * KP + nb);
+          v[0] = fma(l, a0.x, v[0]);
+          v[1] = fma(l, a0.y, v[1]);
+          v[2] = fma(l, a1.x, v[2]);
+          v[3] = fma(l, a1.y, v[3]);
+        }
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) bn[cc] = sc * v[cc];
+      }
+      double bf[4], bu[4] = {0.0, 0.0, 0.0, 0.0}, bv[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) bf[cc] = FB[((s * 4 + cc) * NFQ + q) * ES + fl] - bn[cc];
+      roe_flux_vjp(up, um, n.x, n.y, bf, bu, bv);
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) FB[((s * 4 + cc) * NFQ + q) * ES + fl] = bu[cc];
+      if (mirror) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) FB[((s * 4 + cc) * NFQ + qm) * ES + nl] = bv[cc];
+      }
+    }
+    __syncthreads();
+
+    // next tile's metadata (next_run has arrived by now)
+    if (has_next) {
+      nitems = __ldg(a.tile_count + tile + G);
+      my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
+      const int pos = col % kTileRun;
+      const bool second = col >= kTileRun;
+      my_nb = pos < (second ? next_run.w : next_run.y) ? __ldg(a.nbr + (second ? next_run.z : next_run.x) + pos)
+                                                       : make_int4(0, 0, 0, 0);
+    }
+
+    // ---- 4a. trace adjoints onto the side nodes, component c --------------------------
+    double g[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) g[i] = 0.0;
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+      for (int q = 0; q < NFQ; ++q) {
+        const double b = FB[((s * 4 + c) * NFQ + q) * ES + el];
+#pragma unroll
+        for (int k = 0; k < NE; ++k) g[edge_node(P, s, k)] = fma(ops.tp[s][q][k], b, g[edge_node(P, s, k)]);
+      }
+    __syncthreads();
+
+    // ---- 4b. transposed volume operator: rows j*8 + c (xi), j*8 + 4 + c (eta) ---------
+    double* Gs = FB;
+    if (P > 0) {
+      double lam[NP];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) lam[i] = valid ? __ldg(Ad + comp_index(KP, i, c, e)) : 0.0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        double bx = 0.0, by = 0.0;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          bx = fma(ops.D[0][i][j], lam[i], bx);
+          by = fma(ops.D[1][i][j], lam[i], by);
+        }
+        Gs[(j * 8 + c) * ES + el] = bx * sa;
+        Gs[(j * 8 + 4 + c) * ES + el] = by * sa;
+      }
+    }
+    __syncthreads();
+
+    // ---- 5. transposed nodal flux Jacobian of every node, in place over the xi rows ----
+    if (P > 0) {
+      const int eg = valid ? e : run.x;
+      const double2 j0 = __ldg(a.geo + 0 * KP + eg);
+      const double2 j1 = __ldg(a.geo + 1 * KP + eg);
+      for (int j = c; j < NP; j += 4) {
+        const double2 s0 = S[(2 * j) * ES + el], s1 = S[(2 * j + 1) * ES + el];
+        const double sv[4] = {s0.x, s0.y, s1.x, s1.y};
+        double bx[4], by[4], gv[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          bx[cc] = Gs[(j * 8 + cc) * ES + el];
+          by[cc] = Gs[(j * 8 + 4 + cc) * ES + el];
+        }
+        contravariant_vjp(sv, j0.x, j0.y, j1.x, j1.y, bx, by, gv);
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) Gs[(j * 8 + cc) * ES + el] = gv[cc];
+      }
+    }
+    __syncthreads();
+
+    // the state tile is free: start the next tile's copies and neighbour rows
+    if (has_next) {
+      if (t < 32) issue_tile_copies<NP, ES>(a.U, KP, next_run, S, bar, lane);
+      const int pos = col % kTileRun;
+      const bool second = col >= kTileRun;
+      const bool nvalid = pos < (second ? next_run.w : next_run.y);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int rr = grp + 4 * k;
+        hreg[k] = (nvalid && rr < 2 * NE) ? __ldg(a.U + rr * KP + my_nb.x) : make_double2(1.0, 0.0);
+      }
+    }
+
+    // ---- 6. reverse RK combine, component c of every node ------------------------------
+    if (valid) {
+      const double h = a.elem_dt ? __ldg(a.elem_dt + e) : 1.0;
+      const double cl = a.elem_dt ? a.cl * h : a.cl, cg = a.elem_dt ? a.cg * h : a.cg;
+      const bool need_lam = a.lam_coef != 0.0 || a.a_out;
+      const double* lamp = reinterpret_cast<const double*>(a.lam);
+      const double* accp = reinterpret_cast<const double*>(a.acc_in);
+      double* acco = reinterpret_cast<double*>(a.acc_out);
+      double* aout = reinterpret_cast<double*>(a.a_out);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const long long x = comp_index(KP, i, c, e);
+        const double gi = P > 0 ? g[i] + Gs[(i * 8 + c) * ES + el] : g[i];
+        const double l = need_lam ? lamp[x] : 0.0;
+        const double ai = accp ? accp[x] : 0.0;
+        acco[x] = fma(a.lam_coef, l, ai) + gi;
+        if (aout) aout[x] = fma(cl, l, cg * gi);
+      }
+    }
+    run = next_run;
+    __syncthreads();  // the next tile reuses the shared buffers
+  }
+
+  if (*abort_flag) {
+    // the bulk copies of a tile whose wait gave up may still land: wait for
+    // them once more, with the same bound, before the block leaves
+    for (unsigned n = 0; n < kMaxWaitTries; ++n)
+      if (mbar_try_wait(bar, parity ^ 1u)) break;
+  }
+}
+
+}  // namespace vt

@@ -116,9 +116,10 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 constexpr unsigned kMaxWaitTries = 1u << 22;
 
 // Warp 0 issues the bulk copies of a tile's 2*Np state rows (two runs each)
-// into S, after lane 0 announced the byte count on the barrier.
+// of `src` (rows Kpad apart) into S, after lane 0 announced the byte count on
+// the barrier.
 template <int NP, int ES>
-__device__ __forceinline__ void issue_tile_copies(const StageArgs& a, const int4 run, double2* S,
+__device__ __forceinline__ void issue_tile_copies(const double2* src, long long Kpad, const int4 run, double2* S,
                                                   unsigned long long* bar, int lane) {
   const unsigned b0 = static_cast<unsigned>(run.y) * 16u, b1 = static_cast<unsigned>(run.w) * 16u;
   if (lane == 0) {
@@ -130,7 +131,7 @@ __device__ __forceinline__ void issue_tile_copies(const StageArgs& a, const int4
     const int r = l >> 1, which = l & 1;
     const int start = which ? run.z : run.x;
     const unsigned bytes = which ? b1 : b0;
-    if (bytes) bulk_g2s(S + r * ES + which * kTileRun, a.in + r * a.Kpad + start, bytes, bar);
+    if (bytes) bulk_g2s(S + r * ES + which * kTileRun, src + r * Kpad + start, bytes, bar);
   }
 }
 
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       hreg[k] = (valid && r < 2 * NE) ? __ldg(a.in + r * KP + my_nb.x) : make_double2(1.0, 0.0);
     }
   }
-  if (t < 32) issue_tile_copies<NP, ES>(a, run, S, bar, lane);
+  if (t < 32) issue_tile_copies<NP, ES>(a.in, a.Kpad, run, S, bar, lane);
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
 
     // the state tile is free: start the next tile's copies and neighbour rows
     if (has_next) {
-      if (t < 32) issue_tile_copies<NP, ES>(a, next_run, S, bar, lane);
+      if (t < 32) issue_tile_copies<NP, ES>(a.in, a.Kpad, next_run, S, bar, lane);
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       const bool nvalid = pos < (second ? next_run.w : next_run.y);
