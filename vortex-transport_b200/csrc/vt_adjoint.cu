@@ -149,7 +149,7 @@ struct AdjointState {
   double2* bufs = nullptr;
   double2 *work = nullptr, *s1 = nullptr, *s2 = nullptr, *s3 = nullptr;
   double2 *lam = nullptr, *acc = nullptr, *a0 = nullptr, *a1 = nullptr;
-  double2 *bp = nullptr, *bm = nullptr;  // face adjoints
+  double2 *bp = nullptr, *bm = nullptr;  // face adjoints of the two-launch form (else null)
   // fused reverse stage (adjoint_tile_kernel): persistent grid size, 0 when
   // the edge-once form does not apply (the element adjacency does not
   // 2-colour) or the kernel cannot be resident
@@ -173,31 +173,14 @@ int setup(vt_ctx* c) {
   if (c->adj) return VT_OK;
   if (!c->side_pairing)
     return fail(VT_ERR_UNSUPPORTED, "adjoint: side s of some element does not face side s of its neighbour");
-  auto* s = new AdjointState();
-  s->k = select_adjoint(c->p, c->nfq);
-  if (!s->k.face) {
-    delete s;
-    return fail(VT_ERR_UNSUPPORTED, "adjoint: unsupported (p, nfq)");
-  }
-  s->state_elems = static_cast<size_t>(2 * c->Np) * static_cast<size_t>(c->Kpad);
-  const size_t face_elems = static_cast<size_t>(6 * c->nfq) * static_cast<size_t>(c->Kpad);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s->bufs), sizeof(double2) * (8 * s->state_elems + 2 * face_elems));
-  if (!e) e = cudaMemsetAsync(s->bufs, 0, sizeof(double2) * (8 * s->state_elems + 2 * face_elems), c->stream);
-  if (e) {
-    delete s;
-    return fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, cuda_msg("adjoint buffers", e));
-  }
-  double2** named[8] = {&s->work, &s->s1, &s->s2, &s->s3, &s->lam, &s->acc, &s->a0, &s->a1};
-  for (int i = 0; i < 8; ++i) *named[i] = s->bufs + i * s->state_elems;
-  s->bp = s->bufs + 8 * s->state_elems;
-  s->bm = s->bp + face_elems;
-  c->adj = s;
+  const AdjKernels k = select_adjoint(c->p, c->nfq);
+  if (!k.face) return fail(VT_ERR_UNSUPPORTED, "adjoint: unsupported (p, nfq)");
   // The edge-once form needs every edge to join elements whose sides face each
   // other with opposite normals; a 2-colouring of the element adjacency
   // (breadth first) tells such meshes (the reference's type-0 / type-1
   // triangles) from ones with self-neighbours or odd cycles.
   std::vector<int4> nb(static_cast<size_t>(c->K));
-  e = cudaMemcpy(nb.data(), c->nbr, sizeof(int4) * nb.size(), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(nb.data(), c->nbr, sizeof(int4) * nb.size(), cudaMemcpyDeviceToHost);
   if (e) return fail(VT_ERR_CUDA, cuda_msg("adjoint: neighbours", e));
   std::vector<signed char> col(nb.size(), -1);
   std::vector<int> queue;
@@ -219,14 +202,40 @@ int setup(vt_ctx* c) {
       }
     }
   }
+  // the fused reverse stage runs on the stage kernel's tiles
+  int tile_blocks = 0;
   if (ok) {
-    // the fused reverse stage runs on the stage kernel's tiles
     int per_sm = 0, sms = 0;
-    if (c->tiles && c->ntiles > 0 && !s->k.tile_config(&per_sm) &&
+    if (c->tiles && c->ntiles > 0 && !k.tile_config(&per_sm) &&
         !cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) && per_sm > 0)
-      s->tile_blocks = sms * per_sm;
+      tile_blocks = sms * per_sm;
     cudaGetLastError();
   }
+  // eight state vectors, plus the face adjoints of the two-launch form when
+  // that form is the one used
+  const size_t state_elems = static_cast<size_t>(2 * c->Np) * static_cast<size_t>(c->Kpad);
+  const size_t face_elems = tile_blocks > 0 ? 0 : static_cast<size_t>(6 * c->nfq) * static_cast<size_t>(c->Kpad);
+  const size_t total = 8 * state_elems + 2 * face_elems;
+  double2* bufs = nullptr;
+  e = cudaMalloc(reinterpret_cast<void**>(&bufs), sizeof(double2) * total);
+  if (!e) e = cudaMemsetAsync(bufs, 0, sizeof(double2) * total, c->stream);
+  if (e) {
+    if (bufs) cudaFree(bufs);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, cuda_msg("adjoint buffers", e));
+  }
+  auto* s = new AdjointState();
+  s->k = k;
+  s->tile_blocks = tile_blocks;
+  s->state_elems = state_elems;
+  s->bufs = bufs;
+  double2** named[8] = {&s->work, &s->s1, &s->s2, &s->s3, &s->lam, &s->acc, &s->a0, &s->a1};
+  for (int i = 0; i < 8; ++i) *named[i] = s->bufs + i * s->state_elems;
+  if (face_elems) {
+    s->bp = s->bufs + 8 * s->state_elems;
+    s->bm = s->bp + face_elems;
+  }
+  c->adj = s;
   return VT_OK;
 }
 
