@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run here, where the reference sources are mounted (they are not on GPU boxes):
+Run where the reference sources are mounted (the fixtures are committed, so the
+tests themselves never need the sources):
 
     make -C oracle ref            # builds oracle/_ref/vt_ref_harness
     python tests/golden/make_golden.py
