@@ -22,6 +22,16 @@
 
 namespace vt {
 
+// 1/x: recip_nr (vt_device.cuh) in device code, IEEE division on the host, where
+// the reverse sweeps are checked against the dual-number Jacobians.
+__host__ __device__ inline double rcp(double x) {
+#ifdef __CUDA_ARCH__
+  return recip_nr(x);
+#else
+  return 1.0 / x;
+#endif
+}
+
 // ---- dual numbers -------------------------------------------------------------
 template <int N>
 struct Dual {
@@ -172,7 +182,7 @@ __host__ __device__ inline void roe_flux_vjp(const double* uL, const double* uR,
                                              const double* bf, double* buL, double* buR) {
   // forward recomputation of the intermediates
   const double rL = uL[0], rR = uR[0];
-  const double irLR = 1.0 / (rL * rR);
+  const double irLR = rcp(rL * rR);
   const double irL = rR * irLR, irR = rL * irLR;
   const double vxL = uL[1] * irL, vyL = uL[2] * irL;
   const double unL = vxL * nx + vyL * ny;
@@ -186,7 +196,7 @@ __host__ __device__ inline void roe_flux_vjp(const double* uL, const double* uR,
   const double HR = rHR * irR;
   const double du0 = uR[0] - uL[0], du1 = uR[1] - uL[1], du2 = uR[2] - uL[2], du3 = uR[3] - uL[3];
   const double di = sqrt(rR * irL);
-  const double d1 = 1.0 / (1.0 + di);
+  const double d1 = rcp(1.0 + di);
   const double ui = (di * vxR + vxL) * d1;
   const double vi = (di * vyR + vyL) * d1;
   const double Hi = (di * HR + HL) * d1;
@@ -194,7 +204,7 @@ __host__ __device__ inline void roe_flux_vjp(const double* uL, const double* uR,
   const double ucp = ui * nx + vi * ny;
   const double c2 = kGm1 * (Hi - af);
   const double ci = c2 * c2;
-  const double ci1 = 1.0 / ci;
+  const double ci1 = rcp(ci);
   const double eps = 0.1 * ci;
   const double ieps = 10.0 * ci1;
   const double l0r = ucp + ci, l1r = ucp - ci, l3r = ucp;
@@ -373,7 +383,7 @@ __host__ __device__ inline void roe_flux_vjp(const double* uL, const double* uR,
 // bgxi, bgeta: adjoints of the contravariant flux (4 each); adds the state's adjoint to bs.
 __host__ __device__ inline void contravariant_vjp(const double* s, double j00, double j01, double j10, double j11,
                                                   const double* bgxi, const double* bgeta, double* bs) {
-  const double ir = 1.0 / s[0];
+  const double ir = rcp(s[0]);
   const double vx = s[1] * ir, vy = s[2] * ir;
   const double p = kGm1 * (s[3] - 0.5 * (s[1] * vx + s[2] * vy));
   const double rH = s[3] + p;
