@@ -29,6 +29,10 @@
 //             tile's copies are issued;
 //   6. combine acc_out = acc_in + lam_coef lam + g, a_out = cl lam + cg g.
 //
+// As in the stage kernel, from phase 4 on every shared-memory access stays
+// within an element's four threads, so the barriers after phases 4a, 4b and 5
+// are per-run named barriers and each run issues its own next copies.
+//
 // Every wait on the mbarrier is bounded; a wait that gives up sets bit 1 of
 // err[3] and the block stops taking tiles.
 #pragma once
@@ -100,7 +104,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
     for (int l = t; l < 3 * NP * NFQ; l += T) LF[l] = lf[l];
   }
   if (t == 0) {
-    mbar_init(bar, 1);
+    mbar_init(bar, 2);
     *abort_flag = 0;
   }
   __syncthreads();
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       hreg[k] = (valid && r < 2 * NE) ? __ldg(a.U + r * KP + my_nb.x) : make_double2(1.0, 0.0);
     }
   }
-  if (t < 32) issue_tile_copies<NP, ES>(a.U, KP, run, S, bar, lane);
+  if (t < 64) issue_run_copies<NP, ES>(a.U, KP, run, t >> 5, S, bar, lane);
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
 #pragma unroll
         for (int k = 0; k < NE; ++k) g[edge_node(P, s, k)] = fma(ops.tp[s][q][k], b, g[edge_node(P, s, k)]);
       }
-    __syncthreads();
+    run_sync(t);
 
     // ---- 4b. transposed volume operator: rows j*8 + c (xi), j*8 + 4 + c (eta) ---------
     double* Gs = FB;
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
         Gs[(j * 8 + 4 + c) * ES + el] = by * sa;
       }
     }
-    __syncthreads();
+    run_sync(t);
 
     // ---- 5. transposed nodal flux Jacobian of every node, in place over the xi rows ----
     if (P > 0) {
@@ -365,11 +369,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
         for (int cc = 0; cc < 4; ++cc) Gs[(j * 8 + cc) * ES + el] = gv[cc];
       }
     }
-    __syncthreads();
+    run_sync(t);
 
-    // the state tile is free: start the next tile's copies and neighbour rows
+    // this run's columns of the state tile are free: start its next copies and neighbour rows
     if (has_next) {
-      if (t < 32) issue_tile_copies<NP, ES>(a.U, KP, next_run, S, bar, lane);
+      if (t < 64) issue_run_copies<NP, ES>(a.U, KP, next_run, t >> 5, S, bar, lane);
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       const bool nvalid = pos < (second ? next_run.w : next_run.y);

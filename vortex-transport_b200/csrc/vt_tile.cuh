@@ -29,6 +29,13 @@
 //             and the next tile's copies are issued;
 //   6. volume D_xi G_xi + D_eta G_eta, then the RK stage update written back.
 //
+// From phase 4 on, every shared-memory access stays within an element's four
+// threads, which lie in the four warps of equal parity (warps 0, 2, 4, 6 hold
+// the first run's elements, 1, 3, 5, 7 the second's). So the barriers after
+// phases 4 and 5 are per-run 128-thread named barriers, and each run issues its
+// own next copies (the tile's mbarrier expects one arrival per run): the two
+// halves of a block need not wait for each other until the next tile starts.
+//
 // Upcoming rows are also prefetched into L2 (cp.async.bulk.prefetch.L2) one
 // tile ahead and the tile's geometry rows into L1, so no phase waits on HBM.
 // The reference's mass-inverse apply is folded into D and LIFT on the host.
@@ -117,7 +124,7 @@ constexpr unsigned kMaxWaitTries = 1u << 22;
 
 // Warp 0 issues the bulk copies of a tile's 2*Np state rows (two runs each)
 // of `src` (rows Kpad apart) into S, after lane 0 announced the byte count on
-// the barrier.
+// the barrier (which expects one arrival).
 template <int NP, int ES>
 __device__ __forceinline__ void issue_tile_copies(const double2* src, long long Kpad, const int4 run, double2* S,
                                                   unsigned long long* bar, int lane) {
@@ -133,6 +140,30 @@ __device__ __forceinline__ void issue_tile_copies(const double2* src, long long 
     const unsigned bytes = which ? b1 : b0;
     if (bytes) bulk_g2s(S + r * ES + which * kTileRun, src + r * Kpad + start, bytes, bar);
   }
+}
+
+
+// Warp `which` (0 or 1) issues the bulk copies of its run's 2*Np state rows
+// into columns which*32.. of S, after lane 0 announced the run's byte count on
+// the barrier (which expects one arrival per run).
+template <int NP, int ES>
+__device__ __forceinline__ void issue_run_copies(const double2* src, long long Kpad, const int4 run, int which,
+                                                 double2* S, unsigned long long* bar, int lane) {
+  const int start = which ? run.z : run.x;
+  const unsigned bytes = static_cast<unsigned>(which ? run.w : run.y) * 16u;
+  if (lane == 0) {
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, 2u * NP * bytes);
+  }
+  __syncwarp();
+  if (bytes)
+    for (int r = lane; r < 2 * NP; r += 32) bulk_g2s(S + r * ES + which * kTileRun, src + r * Kpad + start, bytes, bar);
+}
+
+// Barrier of the four warps that hold one run's elements (warps of equal parity).
+__device__ __forceinline__ void run_sync(int t) {
+  if ((t >> 5) & 1) asm volatile("bar.sync 2, 128;" ::: "memory");
+  else asm volatile("bar.sync 1, 128;" ::: "memory");
 }
 
 template <int P, int NFQ>
@@ -168,7 +199,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     for (int l = t; l < 3 * NFQ * NE; l += T) TM[l] = tm[l];
   }
   if (t == 0) {
-    mbar_init(bar, 1);
+    mbar_init(bar, 2);
     *abort_flag = 0;
   }
   __syncthreads();
@@ -193,7 +224,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       hreg[k] = (valid && r < 2 * NE) ? __ldg(a.in + r * KP + my_nb.x) : make_double2(1.0, 0.0);
     }
   }
-  if (t < 32) issue_tile_copies<NP, ES>(a.in, a.Kpad, run, S, bar, lane);
+  if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, run, t >> 5, S, bar, lane);
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
@@ -364,7 +395,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
         }
       }
     }
-    __syncthreads();
+    run_sync(t);
 
     // ---- 5. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ---------------
     double* Gs = FB;
@@ -383,11 +414,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
         }
       }
     }
-    __syncthreads();
+    run_sync(t);
 
-    // the state tile is free: start the next tile's copies and neighbour rows
+    // this run's columns of the state tile are free: start its next copies and neighbour rows
     if (has_next) {
-      if (t < 32) issue_tile_copies<NP, ES>(a.in, a.Kpad, next_run, S, bar, lane);
+      if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, next_run, t >> 5, S, bar, lane);
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       const bool nvalid = pos < (second ? next_run.w : next_run.y);
