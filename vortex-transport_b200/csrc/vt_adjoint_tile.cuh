@@ -31,7 +31,11 @@
 //
 // As in the stage kernel, from phase 4 on every shared-memory access stays
 // within an element's four threads, so the barriers after phases 4a, 4b and 5
-// are per-run named barriers and each run issues its own next copies.
+// are per-run named barriers and each run issues its own next copies; the load
+// phase has no block barrier (phase 2 reads only global memory and writes the
+// thread's own column, phase 3 comes after a barrier), and a tile ends with a
+// per-run barrier (the next tile's phase 2 reuses rows that this tile's phase
+// 6 reads in other warps of the same run).
 //
 // Every wait on the mbarrier is bounded; a wait that gives up sets bit 1 of
 // err[3] and the block stops taking tiles.
@@ -189,14 +193,12 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       }
     }
     parity ^= 1u;
-    __syncthreads();
-    if (*abort_flag) break;
 
     // ---- 2. lifted face adjoints bF[s][c][q][el], thread (element el, component c) ----
     const int c = grp;  // uniform per warp
     const int el = col;
-    const int e = EL[el];
-    const bool valid = e >= 0;
+    const bool valid = col % kTileRun < (col >= kTileRun ? run.w : run.y);
+    const int e = valid ? (col >= kTileRun ? run.z : run.x) + col % kTileRun : -1;  // EL[el]
     const double sa = valid && a.elem_dt && a.sa_dt ? a.sa * __ldg(a.elem_dt + e) : a.sa;
     {
       double lam[NP];
@@ -220,6 +222,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       }
     }
     __syncthreads();
+    if (*abort_flag) break;
 
     // ---- 3. faces: transposed Roe Jacobian; the trace adjoints overwrite bF ----------
     for (int w = t; w < nitems * NFQ; w += T) {
@@ -404,7 +407,10 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       }
     }
     run = next_run;
-    __syncthreads();  // the next tile reuses the shared buffers
+    // the four warps of a run hold different components of the same elements:
+    // none may start the next tile's traces (which reuse rows of the face /
+    // flux buffer) before the others are done with this tile's
+    run_sync(t);
   }
 
   if (*abort_flag) {

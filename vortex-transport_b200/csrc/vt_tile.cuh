@@ -33,8 +33,15 @@
 // threads, which lie in the four warps of equal parity (warps 0, 2, 4, 6 hold
 // the first run's elements, 1, 3, 5, 7 the second's). So the barriers after
 // phases 4 and 5 are per-run 128-thread named barriers, and each run issues its
-// own next copies (the tile's mbarrier expects one arrival per run): the two
-// halves of a block need not wait for each other until the next tile starts.
+// own next copies (the tile's mbarrier expects one arrival per run). The load
+// phase has no block barrier either: the traces read only the thread's own
+// column of the state tile, which its own wait on the mbarrier covers, and the
+// face list, neighbour rows and element indices written there are first read
+// in phase 3, after the barrier that follows the traces. A tile ends with a
+// per-run barrier: the four warps of a run hold different components of the
+// same elements, and the next tile's traces reuse rows of the buffer that this
+// tile's volume phase reads. So the two halves of a block run apart from phase
+// 4 of one tile to the end of the next tile's trace phase.
 //
 // Upcoming rows are also prefetched into L2 (cp.async.bulk.prefetch.L2) one
 // tile ahead and the tile's geometry rows into L1, so no phase waits on HBM.
@@ -289,8 +296,6 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       }
     }
     parity ^= 1u;
-    __syncthreads();
-    if (*abort_flag) break;
 
     // ---- 2. own traces: Tr[s][c][q][el], thread (element el, component c) ----------
     {
@@ -310,6 +315,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
         }
     }
     __syncthreads();
+    if (*abort_flag) break;
 
     // ---- 3. faces: the flux overwrites the traces it consumed ----------------------------
     for (int w = t; w < nitems * NFQ; w += T) {
@@ -483,7 +489,10 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       }
     }
     run = next_run;
-    __syncthreads();  // the next tile reuses the shared buffers
+    // the four warps of a run hold different components of the same elements:
+    // none may start the next tile's traces (which reuse rows of the face /
+    // flux buffer) before the others are done with this tile's
+    run_sync(t);
   }
 
   if (*abort_flag) {
