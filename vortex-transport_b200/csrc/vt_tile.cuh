@@ -129,27 +129,6 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 
 constexpr unsigned kMaxWaitTries = 1u << 22;
 
-// Warp 0 issues the bulk copies of a tile's 2*Np state rows (two runs each)
-// of `src` (rows Kpad apart) into S, after lane 0 announced the byte count on
-// the barrier (which expects one arrival).
-template <int NP, int ES>
-__device__ __forceinline__ void issue_tile_copies(const double2* src, long long Kpad, const int4 run, double2* S,
-                                                  unsigned long long* bar, int lane) {
-  const unsigned b0 = static_cast<unsigned>(run.y) * 16u, b1 = static_cast<unsigned>(run.w) * 16u;
-  if (lane == 0) {
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(bar, 2u * NP * (b0 + b1));
-  }
-  __syncwarp();
-  for (int l = lane; l < 4 * NP; l += 32) {
-    const int r = l >> 1, which = l & 1;
-    const int start = which ? run.z : run.x;
-    const unsigned bytes = which ? b1 : b0;
-    if (bytes) bulk_g2s(S + r * ES + which * kTileRun, src + r * Kpad + start, bytes, bar);
-  }
-}
-
-
 // Warp `which` (0 or 1) issues the bulk copies of its run's 2*Np state rows
 // into columns which*32.. of S, after lane 0 announced the run's byte count on
 // the barrier (which expects one arrival per run).
