@@ -1,7 +1,7 @@
 """Batched adjoint and the batched inverse problem (vt_batch_adjoint_*):
 
 * the reverse sweep over a batch group equals, bit for bit, each instance's
-  reverse sweep on its own solver (same tiles, same owners, same kernels),
+  reverse sweep on its own solver (same tiles, same face lists, same kernels),
   with one or several time steps among the instances;
 * recovering (eps, M, x0, y0) of several vortices from their final states by
   per-instance L-BFGS on batched gradients converges to the true parameters.
