@@ -7,8 +7,9 @@
 // per stage:
 //
 //   1. load   the tile's state rows arrive in shared memory by TMA bulk copies
-//             (cp.async.bulk, completion on an mbarrier) issued during the
-//             previous tile's volume phase; the side-0 neighbours' side nodes,
+//             (cp.async.bulk, completion on an mbarrier), each run's issued
+//             when that run finished the previous tile's flux phase; the
+//             side-0 neighbours' side nodes,
 //             the neighbour table and the tile's face list were loaded into
 //             registers during the previous tile as well;
 //   2. traces 4 threads per element, one conserved component each, evaluate
