@@ -26,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "vt_ref_harness")
-SHIPPED_INPUT = "/root/reference/input_files/input"
+SHIPPED_INPUT = os.path.join(os.environ.get("VT_REFERENCE_SRC", "/root/reference"), "input_files", "input")
 
 # name -> harness arguments
 CASES = {

@@ -15,10 +15,10 @@ pytestmark = pytest.mark.gpu
 
 def test_newton_reciprocal_matches_division(tmp_path):
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    exe = str(tmp_path / "gpu_reciprocal_probe")
+    exe = str(tmp_path / "gpu_reciprocal_check")
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17",
                     "-I", os.path.join(ROOT, "vortex-transport_b200", "csrc"),
-                    os.path.join(ROOT, "tests", "gpu_reciprocal_probe.cu"), "-o", exe],
+                    os.path.join(ROOT, "tests", "gpu_reciprocal_check.cu"), "-o", exe],
                    check=True, capture_output=True, text=True, timeout=600)
     out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=120).stdout
     m = re.search(r"samples (\d+) max_ulp (\d+) differing (\d+)", out)

@@ -99,10 +99,14 @@ __device__ __forceinline__ void record_error(const StageArgs& a, int nfq, int e,
 // terms): the hardware reciprocal estimate (rcp.approx.ftz.f64, relative error
 // about 1e-6 measured on B200) refined by two Newton-Raphson steps
 // r <- r + r (1 - x r), each of which squares the relative error, so the
-// result is within rounding of 1/x; it matched 1.0 / x bit for bit on 2.4
-// million inputs in [2^-10, 2^10] (tests/test_gpu_reciprocal.py). Zero,
-// subnormal and non-finite x are not handled (those states are non-physical
-// and reported by the flux's checks).
+// result is within rounding of 1/x. This is the textbook Newton iteration for
+// the reciprocal with the residual 1 - x r formed by one fused multiply-add,
+// as in P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Develop. 34(1), 1990, and his book
+// "IA-64 and Elementary Functions" (2000), ch. 8. It matched 1.0 / x bit for
+// bit on 2.4 million inputs in [2^-10, 2^10] (tests/test_gpu_reciprocal.py
+// bounds the difference at one ulp). Zero, subnormal and non-finite x are not
+// handled (those states are non-physical and reported by the flux's checks).
 __device__ __forceinline__ double recip_nr(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
