@@ -229,6 +229,17 @@ int vt_read_state_file(const char* path, double* U);
 /* The context's cudaStream_t, for callers that interleave their own work. */
 void* vt_stream(vt_ctx* ctx);
 
+/* Test hook of the stage kernels' bounded waits (no reference counterpart:
+ * the reference has no asynchronous copies). Every wait of a stage kernel on
+ * its tile's bulk copies gives up after a fixed number of polls, records
+ * "a bulk-copy wait gave up" and stops the block, so a lost copy cannot hang
+ * the GPU. tries > 0 sets that bound for the context's later steps;
+ * issue_no_copies != 0 makes the kernels issue no state copies at all, so
+ * every wait gives up (with no copy in flight) and vt_step_rk4 returns
+ * VT_ERR_CUDA with the state unchanged. vt_test_bulk_wait(ctx, 0, 0) restores
+ * the defaults; the context then steps as before. */
+int vt_test_bulk_wait(vt_ctx* ctx, unsigned tries, int issue_no_copies);
+
 /* Device time of each kernel kind of one RK4 step, measured with CUDA events
  * around individual launches (no graph): ms[0..3] = stages 0..3, averaged over
  * `reps` steps of size dt. Advances the state by `reps` steps. */
@@ -387,11 +398,16 @@ size_t vt_noalloc_scratch_bytes(int p, int n_elements);
  * the default stream), the same kernels as vt_step_rk4, with no cudaMalloc,
  * cudaFree or allocating library call. Blocks until done. Returns VT_OK, a
  * non-physical-state code with `err` filled in, VT_ERR_INVALID for a problem
- * larger than the scratch or a bad neighbour index, or VT_ERR_CUDA.
- * The first call on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress) with that device current, so make that first call
+ * larger than the scratch, a bad neighbour index or a misaligned array (dU_in
+ * and dU_out 16-byte aligned, the mesh's doubles 8 and ints 4; checked before
+ * any device work), or VT_ERR_CUDA.
+ * Every call looks up the scratch array's device address on the current device
+ * (cudaGetSymbolAddress: a lookup, not an allocation), so the address is never
+ * stale, not even after cudaDeviceReset; the first call on a device also reads
+ * its SM count and may load the library's kernels, so make that first call
  * before any stream capture. Every call shares the one array and leaves its
- * contents behind; calls whose work overlaps on the GPU race on it. */
+ * contents behind (each call clears the words that must start at zero); calls
+ * whose work overlaps on the GPU race on it. */
 int vt_step_rk4_noalloc(const vt_device_mesh* mesh, const double* dU_in, double* dU_out, double dt,
                         int nsteps, void* stream, vt_error_info* err);
 

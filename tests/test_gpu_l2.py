@@ -57,5 +57,14 @@ def test_config1_l2_against_translated_vortex(vt):
     s.rk4(g.meta["dt"], 10000)
     got = s.l2_error(exact, pb.array("area_quad"))
     np.testing.assert_allclose(got, oracle_l2(pb, exact, s.download()), rtol=1e-12)
-    print("config 1 L2 error vs the translated vortex:", got, "reference script (io=6):", REFERENCE_L2)
-    assert np.all(got < 10 * np.array(REFERENCE_L2))
+    # The reference's own L2 error: its 10000-step state (the fixture, written
+    # by the reference build) against the same exact state, through the oracle's
+    # restatement of its script. An error norm amplifies relative differences
+    # of the state (the state differs from the reference's by <= 1e-9 relative
+    # per node, measured ~4e-14, while the error is ~1e-4 of the state), so the
+    # bar is absolute: the two L2 errors agree to 1e-11 (and to 1e-7 relative).
+    ref_l2 = oracle_l2(pb, exact, g["U_final"])
+    print("config 1 L2 error vs the translated vortex:", got, "reference's own state:", ref_l2,
+          "difference:", np.abs(got - ref_l2), "reference script (io=6, 6-digit dumps):", REFERENCE_L2)
+    np.testing.assert_allclose(got, ref_l2, rtol=1e-7, atol=1e-11)
+    assert np.max(np.abs(got - ref_l2)) < 1e-11

@@ -93,3 +93,89 @@ def test_noalloc_rejects_problems_larger_than_the_scratch(vt):
                                       ctypes.c_void_p(U.data_ptr()), 1e-3, 1, None, ctypes.byref(err))
     assert st == vt.VT_ERR_INVALID
     assert "scratch" in vt._message()
+
+
+def _call(vt, mesh, src, dst, dt, n):
+    err = vt.vt_error_info()
+    st = vt.lib().vt_step_rk4_noalloc(ctypes.byref(mesh), ctypes.c_void_p(src.data_ptr()),
+                                      ctypes.c_void_p(dst.data_ptr()), dt, n, None, ctypes.byref(err))
+    return st, err
+
+
+def test_noalloc_call_takes_no_device_memory(vt):
+    """After a first call (which may load the kernels), a call leaves the
+    device's free memory exactly as it was: nothing is allocated or freed."""
+    import torch
+
+    pb = vt.Problem(vt.make_params(16, 16, p=3, integration_order=10, perturb_grid=0.2))
+    mesh, keep = device_mesh(vt, pb)
+    U = torch.from_numpy(pb.array("U0")).cuda()
+    V = torch.empty_like(U)
+    torch.cuda.synchronize()
+    assert _call(vt, mesh, U, V, 1e-3, 2)[0] == vt.VT_OK, vt._message()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    assert _call(vt, mesh, V, U, 1e-3, 2)[0] == vt.VT_OK, vt._message()
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+
+
+def test_noalloc_in_place_matches_regular_stepper(vt):
+    """dU_in and dU_out may be the same buffer."""
+    import torch
+
+    pb = vt.Problem(vt.make_params(16, 16, p=3, integration_order=10, perturb_grid=0.2))
+    mesh, keep = device_mesh(vt, pb)
+    U = torch.from_numpy(pb.array("U0")).cuda()
+    torch.cuda.synchronize()
+    st, _ = _call(vt, mesh, U, U, 1e-3, 3)
+    assert st == vt.VT_OK, vt._message()
+    ref = vt.Solver(pb)
+    ref.rk4(1e-3, 3)
+    want = ref.download()
+    ref.close()
+    assert float(np.max(np.abs(U.cpu().numpy() - want) / np.abs(want))) < STATE_RTOL
+
+
+def test_noalloc_reports_a_nonphysical_state_like_the_regular_stepper(vt):
+    """A planted negative density stops the step with the same code and the
+    same first failing element, face point, side, step and stage as
+    vt_step_rk4 reports through vt_last_error."""
+    import torch
+
+    pb = vt.Problem(vt.make_params(16, 16, p=2, integration_order=10))
+    mesh, keep = device_mesh(vt, pb)
+    U0 = pb.array("U0").copy()
+    U0[37, 2, 0] = -0.5
+    U = torch.from_numpy(U0).cuda()
+    V = torch.empty_like(U)
+    torch.cuda.synchronize()
+    st, err = _call(vt, mesh, U, V, 1e-3, 2)
+    ref = vt.Solver(pb)
+    ref.upload(U0)
+    with pytest.raises(vt.NonPhysicalState) as exc:
+        ref.rk4(1e-3, 2)
+    ref.close()
+    want = exc.value
+    assert st == want.status
+    assert (err.code, err.element, err.point, err.side, err.step, err.stage) == \
+        (want.code, want.element, want.point, want.side, want.step, want.stage)
+
+
+def test_noalloc_rejects_a_neighbour_index_out_of_range(vt):
+    """A neighbour index outside 0..K-1 in the caller's device arrays is found
+    on the device (the packing kernel keeps every access in bounds) and
+    reported as VT_ERR_INVALID."""
+    import torch
+
+    pb = vt.Problem(vt.make_params(16, 16, p=3, integration_order=10))
+    mesh, keep = device_mesh(vt, pb)
+    keep["conn"][5, 1] = pb.K + 7
+    mesh.neighbours = ctypes.c_void_p(keep["conn"].data_ptr())
+    U = torch.from_numpy(pb.array("U0")).cuda()
+    V = torch.empty_like(U)
+    torch.cuda.synchronize()
+    st, _ = _call(vt, mesh, U, V, 1e-3, 1)
+    assert st == vt.VT_ERR_INVALID
+    assert "neighbour" in vt._message()

@@ -150,6 +150,7 @@ _SIGNATURES = {
     "vt_set_time": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vt_totals": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "vt_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "vt_test_bulk_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int]),
     "vt_profile_rk4_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_float)]),
     "vt_batch_create": (ctypes.c_void_p, [ctypes.POINTER(vt_mesh_desc), ctypes.c_int, ctypes.c_int,

@@ -501,6 +501,8 @@ int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
 
 int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int device_pointers) {
   if (!c || !dJdU_T || !dJdU_0) return fail(VT_ERR_INVALID, "vt_adjoint_backward: null argument");
+  if (device_pointers && !(vt::aligned_to(dJdU_T, 16) && vt::aligned_to(dJdU_0, 16)))
+    return fail(VT_ERR_INVALID, "vt_adjoint_backward: device arrays must be 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");
@@ -549,6 +551,8 @@ int vt_adjoint_info(const vt_ctx* c, vt_checkpoint_info* out) {
 
 int vt_rhs_jvp(vt_ctx* c, const double* U, const double* V, double* dR, int device_pointers) {
   if (!c || !U || !V || !dR) return fail(VT_ERR_INVALID, "vt_rhs_jvp: null argument");
+  if (device_pointers && !(vt::aligned_to(U, 16) && vt::aligned_to(V, 16) && vt::aligned_to(dR, 16)))
+    return fail(VT_ERR_INVALID, "vt_rhs_jvp: device arrays must be 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   int st = vt::prepare(c);
@@ -565,6 +569,8 @@ int vt_rhs_jvp(vt_ctx* c, const double* U, const double* V, double* dR, int devi
 
 int vt_rhs_vjp(vt_ctx* c, const double* U, const double* W, double* G, int device_pointers) {
   if (!c || !U || !W || !G) return fail(VT_ERR_INVALID, "vt_rhs_vjp: null argument");
+  if (device_pointers && !(vt::aligned_to(U, 16) && vt::aligned_to(W, 16) && vt::aligned_to(G, 16)))
+    return fail(VT_ERR_INVALID, "vt_rhs_vjp: device arrays must be 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   int st = vt::prepare(c);
@@ -586,6 +592,8 @@ int vt_rhs_vjp(vt_ctx* c, const double* U, const double* W, double* G, int devic
 
 int vt_tangent_rk4(vt_ctx* c, double dt, int nsteps, const double* dU_0, double* dU_T, int device_pointers) {
   if (!c || nsteps < 0 || !dU_0 || !dU_T) return fail(VT_ERR_INVALID, "vt_tangent_rk4: bad argument");
+  if (device_pointers && !(vt::aligned_to(dU_0, 16) && vt::aligned_to(dU_T, 16)))
+    return fail(VT_ERR_INVALID, "vt_tangent_rk4: device arrays must be 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   if (c->pending_steps) return fail(VT_ERR_INVALID, "a previous async step is not synchronised");

@@ -493,6 +493,7 @@ int vt_batch_download_state(vt_batch* b, int i, double* U, double* F) {
 
 int vt_batch_upload_state_device(vt_batch* b, int i, const double* dU) {
   if (!b || !dU || i < 0 || i >= b->n) return fail(VT_ERR_INVALID, "vt_batch_upload_state_device: bad argument");
+  if (!vt::aligned_to(dU, 16)) return fail(VT_ERR_INVALID, "vt_batch_upload_state_device: dU is not 16-byte aligned");
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
   vt::Group& G = b->groups[b->group_of[i]];
@@ -507,6 +508,7 @@ int vt_batch_upload_state_device(vt_batch* b, int i, const double* dU) {
 
 int vt_batch_download_state_device(vt_batch* b, int i, double* dU) {
   if (!b || !dU || i < 0 || i >= b->n) return fail(VT_ERR_INVALID, "vt_batch_download_state_device: bad argument");
+  if (!vt::aligned_to(dU, 16)) return fail(VT_ERR_INVALID, "vt_batch_download_state_device: dU is not 16-byte aligned");
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
   vt::Group& G = b->groups[b->group_of[i]];
@@ -626,6 +628,8 @@ int vt_batch_adjoint_backward_device(vt_batch* b, const double* dJdU_T, double* 
 
 static int batch_backward(vt_batch* b, const double* dJdU_T, double* dJdU_0, int device_pointers) {
   if (!b || !dJdU_T || !dJdU_0) return fail(VT_ERR_INVALID, "vt_batch_adjoint_backward: null argument");
+  if (device_pointers && !(vt::aligned_to(dJdU_T, 8) && vt::aligned_to(dJdU_0, 8)))
+    return fail(VT_ERR_INVALID, "vt_batch_adjoint_backward_device: device arrays must be 8-byte aligned");
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
   if (b->views.size() != b->groups.size()) return fail(VT_ERR_INVALID, "vt_batch_adjoint_backward: no forward sweep");

@@ -46,6 +46,9 @@ struct vt_ctx {
   const double* tile_dt = nullptr;
   const double* elem_dt = nullptr;
   vt::AdjointState* adj = nullptr;
+  // vt_test_bulk_wait: the stage kernels' wait bound and test flags
+  unsigned test_wait_tries = 0;
+  int test_flags = 0;
 };
 
 namespace vt {

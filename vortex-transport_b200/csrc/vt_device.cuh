@@ -74,7 +74,14 @@ struct StageArgs {
   int stage;     // 0..3 RK4 stages, 4 forward Euler, 5 right-hand side only
   double c_acc;  // accumulator coefficient
   double c_out;  // output coefficient
+  // Test hook of the bounded waits (vt_test_bulk_wait): polls of the tile's
+  // mbarrier before a wait gives up (0: the default bound), and bit 0 of
+  // test_flags issues no state copies at all, so every wait gives up.
+  unsigned wait_tries = 0;
+  int test_flags = 0;
 };
+
+enum : int { kTestNoCopies = 1 };
 
 constexpr int kTileRun = 32;            // elements per run
 constexpr int kTileElems = 2 * kTileRun;  // elements per tile

@@ -71,6 +71,32 @@ int stage_ops_doubles(int p, int nfq) {
   return 2 * np * np + 3 * np * nfq + 6 * nfq * ne;
 }
 
+void fold_stage_operators(int p, int nfq, const double* minv, const double* stiff, const double* line,
+                          const double* phi_plus, const double* phi_minus, double* ops) {
+  const int Np = np_of_p(p), NE = p + 1;
+  int o = 0;
+  for (int d = 0; d < 2; ++d)
+    for (int i = 0; i < Np; ++i)
+      for (int j = 0; j < Np; ++j) {
+        long double s = 0;
+        for (int k = 0; k < Np; ++k) s += static_cast<long double>(minv[i * Np + k]) * stiff[(d * Np + k) * Np + j];
+        ops[o++] = static_cast<double>(s);
+      }
+  for (int sd = 0; sd < 3; ++sd)
+    for (int i = 0; i < Np; ++i)
+      for (int q = 0; q < nfq; ++q) {
+        long double s = 0;
+        for (int j = 0; j < Np; ++j) s += static_cast<long double>(minv[i * Np + j]) * phi_plus[(sd * Np + j) * nfq + q];
+        ops[o++] = static_cast<double>(s * line[2 * q + 1]);
+      }
+  for (int sd = 0; sd < 3; ++sd)
+    for (int q = 0; q < nfq; ++q)
+      for (int k = 0; k < NE; ++k) ops[o++] = phi_plus[(sd * Np + edge_node(p, sd, k)) * nfq + q];
+  for (int sd = 0; sd < 3; ++sd)
+    for (int q = 0; q < nfq; ++q)
+      for (int k = 0; k < NE; ++k) ops[o++] = phi_minus[(sd * Np + edge_node(p, sd, k)) * nfq + q];
+}
+
 std::vector<int4> structured_tile_runs(int K, const int32_t* type, const int32_t* conn) {
   return structured_tiles(K, type, conn);
 }

@@ -27,6 +27,15 @@ StageKernel select_kernel(int p, int nfq);
 // Number of doubles of the StageOps<P, NFQ> block for (p, nfq).
 int stage_ops_doubles(int p, int nfq);
 
+// Writes the StageOps<P, NFQ> block (stage_ops_doubles(p, nfq) doubles) into
+// `ops`: M_ref^-1 folded into the volume operators (D = M_ref^-1 S_xi, S_eta)
+// and the lift (M_ref^-1 phi+_s w), with long-double accumulation, and the own /
+// neighbour face tables restricted to each side's p + 1 nodes. The inputs are
+// the reference-space tables of vt_mesh_desc (Preevolve.cpp:15-144,
+// Evolve.cpp:76-132). Host only; allocates nothing.
+void fold_stage_operators(int p, int nfq, const double* minv, const double* stiff, const double* line,
+                          const double* phi_plus, const double* phi_minus, double* ops);
+
 // Two-row tiles for the reference's structured mesh, empty if `conn` is not it.
 std::vector<int4> structured_tile_runs(int K, const int32_t* type, const int32_t* conn);
 // The same runs from the grid size alone (empty unless nx, ny suit them).

@@ -35,12 +35,13 @@ constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-// Per-device set-up: the device address of g_scratch (the host-side symbol is
-// only a stand-in), the kernels' shared-memory attributes and the persistent
-// grid size. Done by the first call on a device, with that device current.
+// Per-device set-up, done by the first call on a device with that device
+// current: the SM count for the persistent grid. The device address of
+// g_scratch (the host-side symbol is only a stand-in) is looked up on every
+// call instead of being cached, so a context re-created after cudaDeviceReset
+// (which may load the module at another address) gets the current one.
 struct DeviceSetup {
   bool done = false;
-  unsigned char* scratch = nullptr;
   int sms = 0;
 };
 DeviceSetup g_setup[kMaxDevices];
@@ -114,35 +115,8 @@ __global__ void scatter_aos_kernel(const double2* __restrict__ soa, double2* __r
 }
 
 // The operator block of StageOps<P, NFQ> (at most 740 doubles), folded on the
-// host into a fixed-size stack buffer.
+// host into a fixed-size stack buffer by the solver's own fold.
 constexpr int kMaxOps = 2 * 10 * 10 + 3 * 10 * 10 + 2 * 3 * 10 * 4;
-
-void fold_ops_fixed(const vt_device_mesh& m, double* ops) {
-  const int p = m.p, Np = np_of(p), NE = p + 1, nfq = m.n_line_points;
-  int o = 0;
-  for (int d = 0; d < 2; ++d)
-    for (int i = 0; i < Np; ++i)
-      for (int j = 0; j < Np; ++j) {
-        long double s = 0;
-        for (int k = 0; k < Np; ++k)
-          s += static_cast<long double>(m.inv_mass_ref[i * Np + k]) * m.stiffness_ref[(d * Np + k) * Np + j];
-        ops[o++] = static_cast<double>(s);
-      }
-  for (int sd = 0; sd < 3; ++sd)
-    for (int i = 0; i < Np; ++i)
-      for (int q = 0; q < nfq; ++q) {
-        long double s = 0;
-        for (int j = 0; j < Np; ++j)
-          s += static_cast<long double>(m.inv_mass_ref[i * Np + j]) * m.phi_plus[(sd * Np + j) * nfq + q];
-        ops[o++] = static_cast<double>(s * m.line_quadrature[2 * q + 1]);
-      }
-  for (int sd = 0; sd < 3; ++sd)
-    for (int q = 0; q < nfq; ++q)
-      for (int k = 0; k < NE; ++k) ops[o++] = m.phi_plus[(sd * Np + edge_node(p, sd, k)) * nfq + q];
-  for (int sd = 0; sd < 3; ++sd)
-    for (int q = 0; q < nfq; ++q)
-      for (int k = 0; k < NE; ++k) ops[o++] = m.phi_minus[(sd * Np + edge_node(p, sd, k)) * nfq + q];
-}
 
 }  // namespace
 }  // namespace vt
@@ -171,6 +145,14 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: the problem needs " + std::to_string(cv.total) +
                                     " bytes of scratch, more than the fixed " +
                                     std::to_string(vt::kScratchBytes) + " (use vt_create for larger meshes)");
+  // the kernels read the states as double2 and the mesh arrays as doubles / ints:
+  // reject misaligned views before any device work
+  if (!vt::aligned_to(dU_in, 16) || !vt::aligned_to(dU_out, 16))
+    return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: dU_in and dU_out must be 16-byte aligned");
+  if (!vt::aligned_to(m->element_type, 4) || !vt::aligned_to(m->neighbours, 4) ||
+      !vt::aligned_to(m->det_jacobian, 8) || !vt::aligned_to(m->inv_jacobian, 8) ||
+      !vt::aligned_to(m->normals, 8) || !vt::aligned_to(m->side_lengths, 8))
+    return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: a mesh array is misaligned for its element type");
   const vt::StageKernel pk = vt::select_kernel(m->p, m->n_line_points);
 
   int dev = 0;
@@ -181,20 +163,22 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
   {
     std::lock_guard<std::mutex> lk(vt::g_setup_mu);
     if (!ds->done) {
-      void* ptr = nullptr;
-      e = cudaGetSymbolAddress(&ptr, vt::g_scratch);
-      if (e) return fail(VT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       e = cudaDeviceGetAttribute(&ds->sms, cudaDevAttrMultiProcessorCount, dev);
       if (e) return fail(VT_ERR_CUDA, std::string("device attribute: ") + cudaGetErrorString(e));
-      ds->scratch = static_cast<unsigned char*>(ptr);
       ds->done = true;
     }
   }
+  // the device address of the scratch array on the current device (a lookup,
+  // no allocation); the host-side symbol g_scratch is only a stand-in
+  void* scratch_ptr = nullptr;
+  e = cudaGetSymbolAddress(&scratch_ptr, vt::g_scratch);
+  if (e || !scratch_ptr)
+    return fail(VT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   int per_sm = 0;
   if ((e = pk.configure(&per_sm))) return fail(VT_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
   const int max_blocks = ds->sms * (per_sm > 0 ? per_sm : 1);
 
-  unsigned char* base = ds->scratch;
+  unsigned char* base = static_cast<unsigned char*>(scratch_ptr);
   auto* errw = reinterpret_cast<unsigned long long*>(base + cv.err);
   auto* geo = reinterpret_cast<double2*>(base + cv.geo);
   auto* nbr = reinterpret_cast<int4*>(base + cv.nbr);
@@ -209,7 +193,8 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
   const int K = m->n_elements, Np = vt::np_of(m->p);
 
   double ops[vt::kMaxOps];
-  vt::fold_ops_fixed(*m, ops);
+  vt::fold_stage_operators(m->p, m->n_line_points, m->inv_mass_ref, m->stiffness_ref, m->line_quadrature,
+                           m->phi_plus, m->phi_minus, ops);
 
   // error key to "none", step and block counters and the neighbour flag to zero
   if ((e = cudaMemsetAsync(errw, 0xFF, sizeof(unsigned long long), st)) ||
@@ -262,17 +247,7 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
   if (words[3] & 1ull) return fail(VT_ERR_INVALID, "vt_step_rk4_noalloc: neighbour index out of range");
   if (words[3] & 2ull) return fail(VT_ERR_CUDA, "vt_step_rk4_noalloc: a bulk-copy wait gave up");
   if (words[0] == ~0ull) return VT_OK;
-  const unsigned long long epoch = words[0] >> 40;
-  unsigned long long local = words[0] & ((1ull << 40) - 1);
-  vt_error_info info{};
-  info.code = static_cast<int>(local & 3ull);
-  local >>= 2;
-  info.side = static_cast<int>(local % 3ull);
-  local /= 3ull;
-  info.point = static_cast<int>(local % static_cast<unsigned long long>(m->n_line_points));
-  info.element = static_cast<int>(local / static_cast<unsigned long long>(m->n_line_points));
-  info.step = static_cast<int64_t>(epoch / 4);
-  info.stage = static_cast<int>(epoch % 4);
+  const vt_error_info info = vt::decode_error_key(words[0], m->n_line_points);
   if (err) *err = info;
   return fail(info.code, "Non-physical state (code " + std::to_string(info.code) + ") at element " +
                              std::to_string(info.element));

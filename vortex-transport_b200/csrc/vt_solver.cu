@@ -20,36 +20,11 @@
 namespace vt {
 namespace {
 
-// Folds M_ref^-1 into the volume and lift operators and restricts the face
-// tables to each side's nodes, in the layout of StageOps<P, NFQ>.
 std::vector<double> fold_operators(int p, int nfq, const double* minv, const double* stiff,
                                    const double* line, const double* phi_plus,
                                    const double* phi_minus) {
-  const int Np = np_of(p), NE = p + 1;
-  std::vector<double> ops;
-  ops.reserve(2 * Np * Np + 3 * Np * nfq + 6 * nfq * NE);
-  for (int d = 0; d < 2; ++d)
-    for (int i = 0; i < Np; ++i)
-      for (int j = 0; j < Np; ++j) {
-        long double s = 0;
-        for (int k = 0; k < Np; ++k)
-          s += static_cast<long double>(minv[i * Np + k]) * stiff[(d * Np + k) * Np + j];
-        ops.push_back(static_cast<double>(s));
-      }
-  for (int sd = 0; sd < 3; ++sd)
-    for (int i = 0; i < Np; ++i)
-      for (int q = 0; q < nfq; ++q) {
-        long double s = 0;
-        for (int j = 0; j < Np; ++j)
-          s += static_cast<long double>(minv[i * Np + j]) * phi_plus[(sd * Np + j) * nfq + q];
-        ops.push_back(static_cast<double>(s * line[2 * q + 1]));
-      }
-  for (int sd = 0; sd < 3; ++sd)
-    for (int q = 0; q < nfq; ++q)
-      for (int k = 0; k < NE; ++k) ops.push_back(phi_plus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
-  for (int sd = 0; sd < 3; ++sd)
-    for (int q = 0; q < nfq; ++q)
-      for (int k = 0; k < NE; ++k) ops.push_back(phi_minus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
+  std::vector<double> ops(static_cast<size_t>(stage_ops_doubles(p, nfq)));
+  fold_stage_operators(p, nfq, minv, stiff, line, phi_plus, phi_minus, ops.data());
   return ops;
 }
 
@@ -356,6 +331,8 @@ vt::StageArgs stage_args(vt_ctx* c, const double2* in, const double2* base, doub
   a.stage = stage;
   a.c_acc = c_acc;
   a.c_out = c_out;
+  a.wait_tries = c->test_wait_tries;
+  a.test_flags = c->test_flags;
   return a;
 }
 
@@ -386,16 +363,7 @@ int finish(vt_ctx* c, int nsteps, double dt) {
     return fail(VT_ERR_CUDA, "stage kernel: a bulk-copy wait gave up (the state is not valid)");
   const unsigned long long key = words[0];
   if (key == ~0ull) return VT_OK;
-  const unsigned long long epoch = key >> 40;
-  unsigned long long local = key & ((1ull << 40) - 1);
-  c->last.code = static_cast<int>(local & 3ull);
-  local >>= 2;
-  c->last.side = static_cast<int>(local % 3ull);
-  local /= 3ull;
-  c->last.point = static_cast<int>(local % static_cast<unsigned long long>(c->nfq));
-  c->last.element = static_cast<int>(local / static_cast<unsigned long long>(c->nfq));
-  c->last.step = static_cast<int64_t>(epoch / 4);
-  c->last.stage = static_cast<int>(epoch % 4);
+  c->last = vt::decode_error_key(key, c->nfq);
   return fail(c->last.code, "Non-physical state (code " + std::to_string(c->last.code) + ") at element " +
                                 std::to_string(c->last.element) + ", step " + std::to_string(c->last.step) +
                                 ", stage " + std::to_string(c->last.stage));
@@ -728,6 +696,7 @@ void vt_destroy(vt_ctx* c) { release(c); }
 
 int vt_upload_state_device(vt_ctx* c, const double* dU) {
   if (!c || !dU) return fail(VT_ERR_INVALID, "null argument");
+  if (!vt::aligned_to(dU, 16)) return fail(VT_ERR_INVALID, "vt_upload_state_device: dU is not 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   cudaError_t e = aos_to_soa(c, dU, c->U);
@@ -750,6 +719,7 @@ int vt_upload_state(vt_ctx* c, const double* U) {
 
 int vt_download_state_device(vt_ctx* c, double* dU) {
   if (!c || !dU) return fail(VT_ERR_INVALID, "null argument");
+  if (!vt::aligned_to(dU, 16)) return fail(VT_ERR_INVALID, "vt_download_state_device: dU is not 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   cudaError_t e = soa_to_aos(c, c->U, dU);
@@ -898,6 +868,8 @@ int vt_totals(vt_ctx* c, double* out) {
 
 int vt_l2_error(vt_ctx* c, int nq, const double* area_quad, const double* U_ref, int device_pointers, double* out) {
   if (!c || nq < 1 || !area_quad || !U_ref || !out) return fail(VT_ERR_INVALID, "vt_l2_error: bad argument");
+  if (device_pointers && !vt::aligned_to(U_ref, 16))
+    return fail(VT_ERR_INVALID, "vt_l2_error: the device array U_ref is not 16-byte aligned");
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   const int Np = c->Np;
@@ -990,6 +962,19 @@ int vt_load_state(vt_ctx* c, const char* path) {
 }
 
 void* vt_stream(vt_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int vt_test_bulk_wait(vt_ctx* c, unsigned tries, int issue_no_copies) {
+  if (!c) return fail(VT_ERR_INVALID, "vt_test_bulk_wait: null context");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->test_wait_tries = tries;
+  c->test_flags = issue_no_copies ? vt::kTestNoCopies : 0;
+  if (c->rk4_graph) {  // the captured step holds the old kernel arguments
+    cudaGraphExecDestroy(c->rk4_graph);
+    c->rk4_graph = nullptr;
+  }
+  return VT_OK;
+}
 
 int vt_profile_rk4_stages(vt_ctx* c, double dt, int reps, float* ms) {
   if (!c || !ms || reps < 1) return fail(VT_ERR_INVALID, "bad argument");

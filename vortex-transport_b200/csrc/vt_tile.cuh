@@ -51,7 +51,9 @@
 // multiple of 128 bytes do not fall into the same banks.
 //
 // Every wait on the mbarrier is bounded; a wait that gives up sets bit 1 of
-// err[3], and the block stops taking tiles.
+// err[3], and the block stops taking tiles. StageArgs::wait_tries and
+// test_flags (vt_test_bulk_wait) let a test shorten the bound and issue no
+// copies, so that the give-up path runs without any copy in flight.
 #pragma once
 
 #include "vt_device.cuh"
@@ -135,7 +137,8 @@ constexpr unsigned kMaxWaitTries = 1u << 22;
 // the barrier (which expects one arrival per run).
 template <int NP, int ES>
 __device__ __forceinline__ void issue_run_copies(const double2* src, long long Kpad, const int4 run, int which,
-                                                 double2* S, unsigned long long* bar, int lane) {
+                                                 double2* S, unsigned long long* bar, int lane, int test_flags = 0) {
+  if (test_flags & kTestNoCopies) return;  // test hook: nothing arrives, every wait gives up
   const int start = which ? run.z : run.x;
   const unsigned bytes = static_cast<unsigned>(which ? run.w : run.y) * 16u;
   if (lane == 0) {
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   const int lane = t & 31;
   const long long KP = a.Kpad;
   const int G = gridDim.x;
+  const unsigned max_tries = a.wait_tries ? a.wait_tries : kMaxWaitTries;
 
   {
     const double* tm = &ops.tm[0][0][0];
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       hreg[k] = (valid && r < 2 * NE) ? __ldg(a.in + r * KP + my_nb.x) : make_double2(1.0, 0.0);
     }
   }
-  if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, run, t >> 5, S, bar, lane);
+  if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, run, t >> 5, S, bar, lane, a.test_flags);
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     }
     {
       bool ok = false;
-      for (unsigned n = 0; n < kMaxWaitTries && !ok; ++n) ok = mbar_try_wait(bar, parity);
+      for (unsigned n = 0; n < max_tries && !ok; ++n) ok = mbar_try_wait(bar, parity);
       if (!ok) {
         atomicOr(&a.err[3], 2ull);
         *abort_flag = 1;
@@ -404,7 +408,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
 
     // this run's columns of the state tile are free: start its next copies and neighbour rows
     if (has_next) {
-      if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, next_run, t >> 5, S, bar, lane);
+      if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, next_run, t >> 5, S, bar, lane, a.test_flags);
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       const bool nvalid = pos < (second ? next_run.w : next_run.y);
@@ -478,7 +482,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   if (*abort_flag) {
     // the bulk copies of a tile whose wait gave up may still land: wait for
     // them once more, with the same bound, before the block leaves
-    for (unsigned n = 0; n < kMaxWaitTries; ++n)
+    for (unsigned n = 0; n < max_tries; ++n)
       if (mbar_try_wait(bar, parity ^ 1u)) break;
   }
   if (a.stage == 3 || a.stage == kStageEuler) {
