@@ -10,10 +10,14 @@
 //
 // On the first call it packs what the element loop reads from the Element and
 // Evolve_element arrays into a vt_mesh_desc, creates the device context and
-// uploads U. Each call then advances one step on the GPU and writes U (and F,
-// with the reference's flux formula) back into the Element objects, so the
-// driver's write_output and anything else that reads them sees the same data
-// as after the reference's rk4. Element::time advances by t_step per call.
+// uploads U. Each call then advances one step on the GPU; the state stays on
+// the device. The reference driver reads the Element objects only when it
+// dumps them (write_output, main.cpp:172-178), so the driver's write_output
+// call sites are redirected as well (-Dwrite_output=vt_write_output_dropin,
+// adapter/Makefile): before a dump, U (and F, with the reference's flux
+// formula) and Element::time are written back into the Element objects, and
+// the reference's own write_output then writes them. A driver that reads the
+// Elements at other times calls vt_dropin_sync(elements) first.
 //
 // The reference-space operators are not stored in Element; they are recovered
 // from element 0's physical ones, which the reference builds as
@@ -28,6 +32,7 @@
 
 #include "Element.H"
 #include "Evolve.H"
+#include "Utilities.H"
 #include "vortex_b200.h"
 
 namespace {
@@ -36,6 +41,7 @@ struct Dropin {
   vt_ctx* ctx = nullptr;
   const Element* elements = nullptr;
   int K = 0, Np = 0, p = 0;
+  bool stale = false;  // the device state is ahead of the Element objects
   std::vector<double> U, F;
 };
 
@@ -144,6 +150,7 @@ void write_back(Element* el) {
     }
     el[n].time = t;
   }
+  g.stale = false;
 }
 
 void step(Element* el, Evolve_element* ev, double dt, int K, bool rk4) {
@@ -160,10 +167,21 @@ void step(Element* el, Evolve_element* ev, double dt, int K, bool rk4) {
     std::exit(EXIT_FAILURE);
   }
   if (st != VT_OK) fail_exit(rk4 ? "vt_step_rk4" : "vt_step_euler");
-  write_back(el);
+  g.stale = true;
 }
 
 }  // namespace
+
+void vt_dropin_sync(Element* elemts) {
+  if (g.ctx && g.stale && g.elements == elemts) write_back(elemts);
+}
+
+// The driver's dumps: bring the Element objects up to date from the device,
+// then the reference's own writer (Utilities.cpp:65-77).
+void vt_write_output_dropin(Element* elemts, const int& total_num_elements, const int& step_num) {
+  vt_dropin_sync(elemts);
+  write_output(elemts, total_num_elements, step_num);
+}
 
 void vt_rk4_dropin(Element* elemts, Evolve_element* evo_elemts, double& t_step, const int& n_elements) {
   step(elemts, evo_elemts, t_step, n_elements, true);
