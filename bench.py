@@ -10,7 +10,7 @@ through one RK stage, so a step is K*Np*4 DOF-stages.
 
 --impl reference times the reference's own CPU code (oracle/_ref, the
 reference compiled from its sources with -O2 -fopenmp) with all host threads on
-a bounded sample of the same per-element work. With N>1 (torchrun) every rank
+the same 768x768 mesh (W untimed, then K timed RK4 steps). With N>1 (torchrun) every rank
 advances its own replica of the headline problem (it needs no collective), the
 ensemble and inverse-problem instances are split over the ranks
 (workloads.partition, no exchange), and rank 0 prints one JSON line.
@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -41,7 +42,9 @@ WORKLOAD = (f"isentropic vortex, {NX}x{NY} cells ({2 * NX * NY:,} triangles), p=
 METRIC = "FP64 DOF-stages/s p=3"
 UNIT = "DOF-stages/s"
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "vt_ref_harness")
-CPU_SAMPLE_CELLS = 256  # 131,072 triangles, the reference's own OpenMP performance mesh size
+# single-thread sample: the same per-element work on 256x256 cells (131,072
+# triangles, the reference's own OpenMP performance mesh size)
+CPU_1T_CELLS = 256
 
 
 def load_peaks():
@@ -125,27 +128,38 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def run_reference_harness(cells: int, steps: int, threads: int):
+def run_reference_harness(cells: int, steps: int, threads: int, warmup: int = 0):
+    """The reference's own code (oracle/_ref/vt_ref_harness: its translation
+    units and its time loop without the text dumps) on `cells` x `cells`;
+    `warmup` untimed steps, then `steps` timed ones."""
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores",
                OMP_SCHEDULE="static", OMP_DYNAMIC="false")
     out = subprocess.run([HARNESS, "--nx", str(cells), "--ny", str(cells), "--p", str(P), "--io",
                           str(IO), "--perturb", str(PERTURB), "--dt", str(DT), "--steps", str(steps),
-                          "--no-ops", "--time"], env=env, capture_output=True, text=True, check=True)
+                          "--warmup", str(warmup), "--no-ops", "--time"], env=env, capture_output=True,
+                         text=True, check=True)
     return json.loads(out.stdout.strip().splitlines()[-1])
 
 
-def cpu_baseline(budget_s: float = 20.0):
-    """The reference's own code timed on this host's cores on a bounded sample."""
+def cpu_baseline():
+    """The reference's own code timed on this host's cores: all threads on the
+    headline mesh itself (768x768, 2 timed RK4 steps after 1 untimed, about 20 s
+    of CPU work), and one thread on a 256x256 sample of the same per-element
+    work (1 RK4 step)."""
     threads = os.cpu_count() or 1
     if os.path.exists(HARNESS):
-        cal = run_reference_harness(CPU_SAMPLE_CELLS, 1, threads)
-        per_step = max(cal["stepping_s"], 1e-3)
-        steps = int(max(1, min(50, budget_s / per_step)))
-        r = run_reference_harness(CPU_SAMPLE_CELLS, steps, threads)
+        r = run_reference_harness(NX, 2, threads, warmup=1)
+        r1 = run_reference_harness(CPU_1T_CELLS, 1, 1)
         return {"value": r["dof_stages_per_s"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                "sample": (f"{steps} RK4 steps of the same per-element work (p={P}, io={IO}, perturb "
-                           f"{PERTURB}, dt {DT}) on {CPU_SAMPLE_CELLS}x{CPU_SAMPLE_CELLS} cells "
-                           f"({2 * CPU_SAMPLE_CELLS ** 2:,} triangles); reference -O2 -fopenmp build")}
+                "same_config": True,
+                "sample": (f"2 timed RK4 steps (after 1 untimed) of the headline workload itself "
+                           f"({NX}x{NY} cells, p={P}, io={IO}, perturb {PERTURB}, dt {DT}); reference "
+                           f"-O2 -fopenmp build, {r['threads']} threads"),
+                "init_s": r["init_s"],
+                "single_thread": {"value": r1["dof_stages_per_s"], "unit": UNIT, "cores": 1,
+                                  "sample": (f"1 RK4 step of the same per-element work on {CPU_1T_CELLS}x"
+                                             f"{CPU_1T_CELLS} cells ({2 * CPU_1T_CELLS ** 2:,} triangles), "
+                                             "OMP_NUM_THREADS=1")}}
     # the C restatement when the reference build is absent
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import vt_oracle
@@ -312,12 +326,15 @@ def adjoint(vt, steps: int = 2000, snapshots=None, device: int = 0):
 def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0, rank: int = 0, world: int = 1,
                     pg=None):
     """The batched adjoint inverse problem: n vortices on 64x64 cells (8,192
-    triangles), p=2, 300 RK4 steps; seeded true (eps, M, x0, y0) and a
-    perturbed guess; per-instance L-BFGS on the host with every loss
-    evaluation one batched forward + reverse sweep (every step start kept).
-    The time step is the ensemble's stability rule at the lowest Mach number
-    the search may try (0.25): 3.65e-5 (1.5e-4 blows up there, as it does in
-    the reference: the Roe dissipation speed is c^4 = M^-4 = 256).
+    triangles), p=2, observed at the configured horizon T = 300 x 1.5e-4 =
+    0.045; seeded true (eps, M, x0, y0) and a perturbed guess; per-instance
+    L-BFGS on the host with every loss evaluation one batched forward + reverse
+    sweep (400 step starts kept on the binomial schedule, the rest recomputed).
+    The configured dt = 1.5e-4 blows up at the
+    lowest Mach number the search may try (0.25), as it does in the reference
+    (its Roe dissipation speed is c^4 = M^-4 = 256; tests/test_inverse_time_step.py
+    shows it on the oracle), so T is reached in 1234 steps of 0.045 / 1234 =
+    3.647e-5, below the ensemble's stability rule at M = 0.25.
 
     With several ranks each solves its share of the vortices (the problems
     are independent); the solve time is the slowest rank's and the per-vortex
@@ -330,9 +347,14 @@ def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0, ran
     guess_all = inverse.perturbed_guess(theta_all, seed=6)
     mine = workloads.partition([1.0] * n, world)[rank]
     theta, guess = theta_all[mine], guess_all[mine]
-    dt = workloads.stable_dt(64, 2, float(inverse.LOWER[1]))
+    horizon = 300 * 1.5e-4
+    steps = int(math.ceil(horizon / workloads.stable_dt(64, 2, float(inverse.LOWER[1]))))
+    dt = horizon / steps
     t0 = time.perf_counter()
-    inv = inverse.BatchedInverse(theta, side=64, p=2, steps=300, dt=dt, device=device)
+    # 400 stored step starts (80 GB for the 128 instances) on the binomial
+    # schedule: every step start (1234, 248 GB) would not fit in HBM
+    inv = inverse.BatchedInverse(theta, side=64, p=2, steps=steps, dt=dt, nsnapshots=min(steps, 400),
+                                 device=device)
     setup_s = max_over_ranks(time.perf_counter() - t0, pg)
     torch.cuda.synchronize()
     if pg:
@@ -349,9 +371,12 @@ def inverse_problem(vt, iterations: int = 50, n: int = 128, device: int = 0, ran
     else:
         got = [local]
     err0, err, done_all, ratio = (np.concatenate([g[k] for g in got]) for k in ("err0", "err", "done", "ratio"))
-    out = {"workload": f"{n} vortices, 64x64 cells (8,192 triangles) each, p=2, io=10, 300 RK4 steps at "
-                       f"dt={dt:.4g}; true eps~U[0.15,0.45], M~U[0.3,0.6], centre~U[-1.5,1.5]^2 (seed 5); "
-                       "guess eps/M +-0.05, centre +-0.3 (seed 6)",
+    out = {"workload": f"{n} vortices, 64x64 cells (8,192 triangles) each, p=2, io=10, observed at T={horizon:g} "
+                       f"(300 x 1.5e-4) reached in {steps} RK4 steps of dt={dt:.4g}; true eps~U[0.15,0.45], "
+                       "M~U[0.3,0.6], centre~U[-1.5,1.5]^2 (seed 5); guess eps/M +-0.05, centre +-0.3 (seed 6)",
+           "horizon": horizon, "steps": steps, "dt": dt,
+           "dt_rule": "1.5e-4 blows up at M=0.25 in the reference's scheme (c^4 dissipation speed); "
+                      "dt = T / ceil(T / stable_dt(64, 2, 0.25))",
            "ranks": world, "iterations_max": iterations, "accepted_steps_median": float(np.median(done_all)),
            "evaluations": evaluations, "solve_s": solve_s, "s_per_evaluation": solve_s / evaluations,
            "iterations_per_s": float(np.median(done_all)) / solve_s,
@@ -392,20 +417,18 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/vt_ref_harness was not built "
                           "(needs the reference sources at build time)"}))
         return 0
-    if args.warmup:
-        run_reference_harness(CPU_SAMPLE_CELLS, min(args.warmup, 3), threads)
-    r = run_reference_harness(CPU_SAMPLE_CELLS, args.steps, threads)
+    r = run_reference_harness(NX, args.steps, threads, warmup=args.warmup)
     value = r["dof_stages_per_s"]
-    K_s = 2 * CPU_SAMPLE_CELLS ** 2
-    sample = (f"each step: one RK4 step of the same per-element work (p={P}, io={IO}, perturb "
-              f"{PERTURB}, dt {DT}) on {CPU_SAMPLE_CELLS}x{CPU_SAMPLE_CELLS} cells ({K_s:,} "
-              f"triangles) instead of {NX}x{NY}; reference compiled -O2 -fopenmp")
+    sample = (f"each step: one RK4 step of the headline workload itself ({NX}x{NY} cells, p={P}, io={IO}, "
+              f"perturb {PERTURB}, dt {DT}), {args.warmup} untimed then {args.steps} timed; reference "
+              f"compiled -O2 -fopenmp, {r['threads']} threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * r["stepping_s"] / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: the reference's isentropic-vortex IC on its generated mesh",
-            "config": {"workload": WORKLOAD, "sample": sample},
+            "config": {"workload": WORKLOAD, "elements": 2 * NX * NY, "nodes_per_element": NP,
+                       "sample": sample, "same_config": True, "init_s": r["init_s"]},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -541,9 +564,8 @@ def main():
                     help="RK4 steps of the 512-problem ensemble comparison at N=1 (0 skips it)")
     ap.add_argument("--adjoint-steps", type=int, default=2000,
                     help="RK4 steps of the adjoint/forward time ratio at N=1 (0 skips it)")
-    ap.add_argument("--inverse-iters", type=int, default=0,
-                    help="L-BFGS iterations of the 128-vortex batched inverse problem at N=1 (0 skips it; "
-                         "50 takes a few minutes)")
+    ap.add_argument("--inverse-iters", type=int, default=50,
+                    help="L-BFGS iterations of the 128-vortex batched inverse problem (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

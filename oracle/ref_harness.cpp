@@ -30,6 +30,7 @@
 //   --rhs             dump the RHS (DG_time_derivative_U) of the initial state
 //   --no-ops          skip the per-element operator dumps
 //   --time            print one JSON timing line for the stepping loop
+//   --warmup N        with --time: N untimed steps before the timed --steps
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -127,7 +128,7 @@ int main(int argc, char** argv) {
   parms.stepping_method = 1;
 
   std::string dump_dir, load_dir;
-  int dump_every = 0;
+  int dump_every = 0, warmup = 0;
   bool want_rhs = false, want_ops = true, want_time = false;
   bool dt_given = false;
   double dt = 0.0;
@@ -159,6 +160,7 @@ int main(int argc, char** argv) {
     else if (!std::strcmp(o, "--rhs")) want_rhs = true;
     else if (!std::strcmp(o, "--no-ops")) want_ops = false;
     else if (!std::strcmp(o, "--time")) want_time = true;
+    else if (!std::strcmp(o, "--warmup")) warmup = std::atoi(next());
     else die((std::string("unknown option ") + o).c_str());
   }
   if (dt_given) parms.time_step = dt;
@@ -340,6 +342,12 @@ int main(int argc, char** argv) {
             r[(static_cast<size_t>(n) * Np + i) * 4 + k] = evolve_elements[n].DG_time_derivative_U[i][k];
       dump_f64(dump_dir, "rhs0", r);
     }
+  }
+
+  // untimed warm-up steps (first touch of the per-step temporaries)
+  for (int a = 0; a < warmup; ++a) {
+    if (parms.stepping_method == 0) forward_euler(elements, evolve_elements, parms.time_step, K);
+    else rk4(elements, evolve_elements, parms.time_step, K);
   }
 
   // ---- time loop: main.cpp:154-170 ----------------------------------------
