@@ -53,30 +53,9 @@ __global__ void batch_soa_to_aos(const double2* __restrict__ soa, double2* __res
 }
 
 std::vector<double> fold(int p, int nfq, const vt_mesh_desc& d) {
-  const int Np = np_of(p), NE = p + 1;
-  std::vector<double> ops;
-  for (int dd = 0; dd < 2; ++dd)
-    for (int i = 0; i < Np; ++i)
-      for (int j = 0; j < Np; ++j) {
-        long double s = 0;
-        for (int k = 0; k < Np; ++k)
-          s += static_cast<long double>(d.inv_mass_ref[i * Np + k]) * d.stiffness_ref[(dd * Np + k) * Np + j];
-        ops.push_back(static_cast<double>(s));
-      }
-  for (int sd = 0; sd < 3; ++sd)
-    for (int i = 0; i < Np; ++i)
-      for (int q = 0; q < nfq; ++q) {
-        long double s = 0;
-        for (int j = 0; j < Np; ++j)
-          s += static_cast<long double>(d.inv_mass_ref[i * Np + j]) * d.phi_plus[(sd * Np + j) * nfq + q];
-        ops.push_back(static_cast<double>(s * d.line_quadrature[2 * q + 1]));
-      }
-  for (int sd = 0; sd < 3; ++sd)
-    for (int q = 0; q < nfq; ++q)
-      for (int k = 0; k < NE; ++k) ops.push_back(d.phi_plus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
-  for (int sd = 0; sd < 3; ++sd)
-    for (int q = 0; q < nfq; ++q)
-      for (int k = 0; k < NE; ++k) ops.push_back(d.phi_minus[(sd * Np + edge_node(p, sd, k)) * nfq + q]);
+  std::vector<double> ops(static_cast<size_t>(stage_ops_doubles(p, nfq)));
+  fold_stage_operators(p, nfq, d.inv_mass_ref, d.stiffness_ref, d.line_quadrature, d.phi_plus, d.phi_minus,
+                       ops.data());
   return ops;
 }
 
@@ -122,6 +101,12 @@ struct vt_batch {
   double2* staging = nullptr;  // largest instance, AoS
   size_t staging_bytes = 0;
   cudaGraphExec_t graph = nullptr;
+  // one stream per group: the groups' stage chains are independent and run as
+  // concurrent branches of the step graph, so one group's wave tail overlaps
+  // the next group's work
+  std::vector<cudaStream_t> gstreams;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
   int sms = 0, per_sm = 0;
   std::vector<double> dt;  // per instance
   int last_instance = -1;
@@ -147,6 +132,11 @@ void release(vt_batch* b) {
   for (double* p : b->view_dt)
     if (p) cudaFree(p);
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (cudaStream_t st : b->gstreams)
+    if (st) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : b->join)
+    if (ev) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
   for (auto& g : b->groups) {
     void* bufs[] = {g.U, g.A, g.Sa, g.Sb, g.geo, g.nbr, g.tiles, g.items, g.count, g.tile_dt, g.err};
     for (void* p : bufs)
@@ -179,20 +169,31 @@ vt::StageArgs group_args(vt::Group& g, const double2* in, double2* out, int stag
   return a;
 }
 
-// one RK4 step of every group; the coefficients are fractions of each tile's dt
+// The four stage launches of one RK4 step of group g on stream st; the
+// coefficients are fractions of each tile's dt.
+cudaError_t enqueue_group_step(vt::Group& g, cudaStream_t st) {
+  const double* ops = g.ops.data();
+  cudaError_t e = g.kern.launch(group_args(g, g.U, g.Sa, 0, 1.0 / 6, 0.5), ops, g.max_blocks, st);
+  if (!e) e = g.kern.launch(group_args(g, g.Sa, g.Sb, 1, 1.0 / 3, 0.5), ops, g.max_blocks, st);
+  if (!e) e = g.kern.launch(group_args(g, g.Sb, g.Sa, 2, 1.0 / 3, 1.0), ops, g.max_blocks, st);
+  if (!e) e = g.kern.launch(group_args(g, g.Sa, g.U, 3, 0.0, 1.0 / 6), ops, g.max_blocks, st);
+  return e;
+}
+
+// One RK4 step of every group. The groups are independent problems: each
+// group's chain of four stages runs on its own stream, forked from and joined
+// back into the batch stream, so that in the captured graph they are parallel
+// branches and the GPU starts one group's blocks while another group's last
+// tiles finish.
 cudaError_t enqueue_step(vt_batch* b) {
-  cudaError_t e = cudaSuccess;
-  for (int st = 0; st < 4 && !e; ++st)
-    for (auto& g : b->groups) {
-      const double* ops = g.ops.data();
-      switch (st) {
-        case 0: e = g.kern.launch(group_args(g, g.U, g.Sa, 0, 1.0 / 6, 0.5), ops, g.max_blocks, b->stream); break;
-        case 1: e = g.kern.launch(group_args(g, g.Sa, g.Sb, 1, 1.0 / 3, 0.5), ops, g.max_blocks, b->stream); break;
-        case 2: e = g.kern.launch(group_args(g, g.Sb, g.Sa, 2, 1.0 / 3, 1.0), ops, g.max_blocks, b->stream); break;
-        default: e = g.kern.launch(group_args(g, g.Sa, g.U, 3, 0.0, 1.0 / 6), ops, g.max_blocks, b->stream); break;
-      }
-      if (e) break;
-    }
+  if (b->groups.size() == 1) return enqueue_group_step(b->groups[0], b->stream);
+  cudaError_t e = cudaEventRecord(b->fork, b->stream);
+  for (size_t gi = 0; gi < b->groups.size() && !e; ++gi) {
+    e = cudaStreamWaitEvent(b->gstreams[gi], b->fork, 0);
+    if (!e) e = enqueue_group_step(b->groups[gi], b->gstreams[gi]);
+    if (!e) e = cudaEventRecord(b->join[gi], b->gstreams[gi]);
+  }
+  for (size_t gi = 0; gi < b->groups.size() && !e; ++gi) e = cudaStreamWaitEvent(b->stream, b->join[gi], 0);
   return e;
 }
 
@@ -362,8 +363,20 @@ vt_batch* vt_batch_create(const vt_mesh_desc* descs, int n, int device, int* sta
     G.K += d.n_elements;
   }
   if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
-      (e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device))) {
+      (e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device)) ||
+      (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming))) {
     set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_create", e)));
+    release(b);
+    return nullptr;
+  }
+  b->gstreams.assign(b->groups.size(), nullptr);
+  b->join.assign(b->groups.size(), nullptr);
+  for (size_t gi = 0; gi < b->groups.size() && !e; ++gi) {
+    e = cudaStreamCreateWithFlags(&b->gstreams[gi], cudaStreamNonBlocking);
+    if (!e) e = cudaEventCreateWithFlags(&b->join[gi], cudaEventDisableTiming);
+  }
+  if (e) {
+    set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_create streams", e)));
     release(b);
     return nullptr;
   }
@@ -553,18 +566,10 @@ int vt_batch_step_rk4(vt_batch* b, int nsteps) {
     if (w[3] & 2ull) return fail(VT_ERR_CUDA, "stage kernel: a bulk-copy wait gave up (the state is not valid)");
     if (w[0] == ~0ull) continue;
     const unsigned long long epoch = w[0] >> 40;
-    unsigned long long local = w[0] & ((1ull << 40) - 1);
-    vt_error_info info{};
-    info.code = static_cast<int>(local & 3ull);
-    local >>= 2;
-    info.side = static_cast<int>(local % 3ull);
-    local /= 3ull;
-    info.point = static_cast<int>(local % static_cast<unsigned long long>(G.nfq));
-    const long long ge = static_cast<long long>(local / static_cast<unsigned long long>(G.nfq));
+    vt_error_info info = vt::decode_error_key(w[0], G.nfq);
+    const long long ge = info.element;  // element of the group's ragged array
     const size_t m = std::upper_bound(G.offset.begin(), G.offset.end(), ge) - G.offset.begin() - 1;
     info.element = static_cast<int>(ge - G.offset[m]);
-    info.step = static_cast<int64_t>(epoch / 4);
-    info.stage = static_cast<int>(epoch % 4);
     const int inst = G.members[m];
     if (epoch < best_epoch || (epoch == best_epoch && inst < b->last_instance)) {
       best_epoch = epoch;
