@@ -228,6 +228,7 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0, rank: int = 0, world
     torch.cuda.synchronize()
     batched_s = max_over_ranks(time.perf_counter() - t0, pg)
     groups = batch.groups
+    group_ms = batch.time_groups(5)  # each group's step on its own, device time
     batch.close()
 
     seq_local = 0.0
@@ -245,6 +246,14 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0, rank: int = 0, world
     bytes_alg = 4 * steps * sum(2 * i.side * i.side * (128 * (i.p + 1) * (i.p + 2) // 2 + 124) for i in inst_all)
     peak, peak_kind = load_peaks()
     achieved = bytes_alg / batched_s / 1e9 / world
+    per_group = []
+    for (gp, gn, gk), ms in zip(groups, group_ms):
+        gnp = (gp + 1) * (gp + 2) // 2
+        rate = gk * gnp * 4 / (ms * 1e-3)
+        gbs = gk * 4 * (128 * gnp + 124) / (ms * 1e-3) / 1e9
+        per_group.append({"p": gp, "instances": gn, "elements": gk, "ms_per_step": ms,
+                          "dof_stages_per_s": rate, "bytes_per_dof_stage": 128 + 124 / gnp,
+                          "hbm_gbs": gbs, "frac": gbs / peak})
     return {
         "workload": (f"{n} seeded vortex problems (seed 1): side in {{16..128}}, p in {{1,2,3}}, "
                      f"eps~U[0.1,0.5], M~U[0.3,0.7], centre~U[-2,2]^2, perturb~U[0,0.2], io=10, "
@@ -255,6 +264,7 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0, rank: int = 0, world
         "ranks": world,
         "instances_per_rank": [len(q) for q in parts],
         "groups": [list(g) for g in groups],
+        "per_group": per_group,
         "blocks_per_sm": tuned,
         "batched_solves_per_s": n / batched_s,
         "sequential_solves_per_s": n / seq_s,

@@ -279,6 +279,11 @@ int vt_batch_last_error(const vt_batch* batch, int* instance, vt_error_info* out
 int vt_batch_autotune(vt_batch* batch, int trials, int* blocks_per_sm);
 /* Applies a stored tuning (as reported by vt_batch_autotune). */
 int vt_batch_set_blocks_per_sm(vt_batch* batch, const int* blocks_per_sm);
+/* Device time of one RK4 step of each group on its own (group order of
+ * vt_batch_group_info), averaged over `reps` steps after one warm-up step; the
+ * groups' states are restored afterwards. No reference counterpart: it
+ * reports how fast each order p runs inside a batch. */
+int vt_batch_time_groups(vt_batch* batch, int reps, float* ms_per_step);
 
 /* ---- discrete adjoint ---------------------------------------------------- */
 /* No counterpart in the reference (which has no derivatives). The exact

@@ -169,6 +169,7 @@ _SIGNATURES = {
                                            ctypes.POINTER(vt_error_info)]),
     "vt_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "vt_batch_set_blocks_per_sm": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "vt_batch_time_groups": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
     "vt_checkpoint_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "vt_save_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "vt_project_vortex": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(vt_vortex), ctypes.c_double,
@@ -817,6 +818,13 @@ class Batch:
             with open(cache, "w") as f:
                 json.dump(data, f, indent=1)
         return best
+
+    def time_groups(self, reps: int = 5) -> list[float]:
+        """Milliseconds per RK4 step of each group run on its own (device time)."""
+        ng = lib().vt_batch_groups(self._h)
+        arr = (ctypes.c_float * ng)()
+        _check(lib().vt_batch_time_groups(self._h, int(reps), arr))
+        return [float(x) for x in arr]
 
     def close(self):
         if getattr(self, "_h", None):

@@ -757,6 +757,35 @@ int vt_batch_autotune(vt_batch* b, int trials, int* blocks_per_sm_out) {
   return capture(b);
 }
 
+int vt_batch_time_groups(vt_batch* b, int reps, float* ms_per_step) {
+  if (!b || reps < 1 || !ms_per_step) return fail(VT_ERR_INVALID, "vt_batch_time_groups: bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) || cudaEventCreate(&e1)) return fail(VT_ERR_CUDA, "vt_batch_time_groups: events");
+  int st = VT_OK;
+  for (size_t gi = 0; gi < b->groups.size() && !st; ++gi) {
+    vt::Group& G = b->groups[gi];
+    // the group's state is saved and restored, so timing does not advance the solution
+    const size_t state = 2 * G.Np * static_cast<size_t>(G.Kpad);
+    std::vector<double2> saved(state);
+    cudaError_t e = cudaMemcpy(saved.data(), G.U, state * sizeof(double2), cudaMemcpyDeviceToHost);
+    if (!e) e = enqueue_group_step(G, b->stream);  // warm-up
+    if (!e) e = cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < reps && !e; ++r) e = enqueue_group_step(G, b->stream);
+    if (!e) e = cudaEventRecord(e1, b->stream);
+    if (!e) e = cudaEventSynchronize(e1);
+    float ms = 0;
+    if (!e) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (!e) e = cudaMemcpy(G.U, saved.data(), state * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e) st = fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_time_groups", e));
+    ms_per_step[gi] = ms / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
 int vt_batch_set_blocks_per_sm(vt_batch* b, const int* blocks_per_sm) {
   if (!b || !blocks_per_sm) return fail(VT_ERR_INVALID, "bad argument");
   std::lock_guard<std::mutex> lk(b->mu);
