@@ -265,7 +265,9 @@ def ensemble(vt, steps: int, n: int = 512, device: int = 0, rank: int = 0, world
         "instances_per_rank": [len(q) for q in parts],
         "groups": [list(g) for g in groups],
         "per_group": per_group,
-        "blocks_per_sm": tuned,
+        "tuning": {"per_group": [{"p": g[0], "blocks_per_sm": b, "mapping": "pair" if m == 1 else "component"}
+                                 for g, (b, m) in zip(groups, tuned)],
+                   "note": "autotuned per group over both warp mappings and 1..3 resident blocks per SM"},
         "batched_solves_per_s": n / batched_s,
         "sequential_solves_per_s": n / seq_s,
         "speedup": seq_s / batched_s,

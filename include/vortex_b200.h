@@ -229,6 +229,13 @@ int vt_read_state_file(const char* path, double* U);
 /* The context's cudaStream_t, for callers that interleave their own work. */
 void* vt_stream(vt_ctx* ctx);
 
+/* Warp mapping of the context's stage kernel: 0 one thread per element and
+ * conserved component, 1 (the default) one thread per element, component pair
+ * and half of the nodes. Both compute the same arithmetic (results agree to
+ * rounding); the choice only changes the speed. No reference counterpart. */
+int vt_set_stage_mapping(vt_ctx* ctx, int mapping);
+int vt_get_stage_mapping(const vt_ctx* ctx);
+
 /* Test hook of the stage kernels' bounded waits (no reference counterpart:
  * the reference has no asynchronous copies). Every wait of a stage kernel on
  * its tile's bulk copies gives up after a fixed number of polls, records
@@ -273,12 +280,16 @@ int vt_batch_set_dt(vt_batch* batch, const double* dt);
  * returns its code; vt_batch_last_error names the instance. */
 int vt_batch_step_rk4(vt_batch* batch, int nsteps);
 int vt_batch_last_error(const vt_batch* batch, int* instance, vt_error_info* out);
-/* Times each group's RK4 step with 1..max resident blocks per SM (`trials`
- * repetitions each), keeps the fastest and reports it per group in
- * blocks_per_sm[groups]; the state is left unchanged. */
-int vt_batch_autotune(vt_batch* batch, int trials, int* blocks_per_sm);
-/* Applies a stored tuning (as reported by vt_batch_autotune). */
+/* Times each group's RK4 step for both warp mappings of the stage kernel
+ * (0: one thread per element and component; 1: one thread per element,
+ * component pair and half of the nodes) and 1..max resident blocks per SM
+ * (`trials` repetitions each), keeps the fastest and reports it per group in
+ * blocks_per_sm[groups] and mapping[groups] (either may be NULL); the state is
+ * left unchanged. No reference counterpart (the reference has one CPU loop). */
+int vt_batch_autotune(vt_batch* batch, int trials, int* blocks_per_sm, int* mapping);
+/* Apply a stored tuning (as reported by vt_batch_autotune). */
 int vt_batch_set_blocks_per_sm(vt_batch* batch, const int* blocks_per_sm);
+int vt_batch_set_mapping(vt_batch* batch, const int* mapping);
 /* Device time of one RK4 step of each group on its own (group order of
  * vt_batch_group_info), averaged over `reps` steps after one warm-up step; the
  * groups' states are restored afterwards. No reference counterpart: it

@@ -61,14 +61,17 @@ def test_batch_autotune_keeps_state_and_caches(vt, tmp_path):
     before = [batch.download(i) for i in range(batch.n)]
     cache = str(tmp_path / "autotune.json")
     best = batch.autotune(trials=2, cache=cache)
-    assert len(best) == len(batch.groups) and all(1 <= b <= 32 for b in best)
+    assert len(best) == len(batch.groups)
+    assert all(1 <= b <= 32 and m in (0, 1) for b, m in best)
     for i in range(batch.n):
         np.testing.assert_array_equal(batch.download(i), before[i])
     again = vt.Batch(pbs).autotune(trials=2, cache=cache)  # read back from the cache
     assert again == best
     batch.rk4(3)
+    mapping_of_p = {g[0]: m for g, (_, m) in zip(batch.groups, best)}
     for i, pb in enumerate(pbs):
         s = vt.Solver(pb)
+        s.stage_mapping = mapping_of_p[pb.p]  # the same kernel as the instance's group
         s.rk4(dts[i], 3)
         np.testing.assert_array_equal(batch.download(i), s.download())
 

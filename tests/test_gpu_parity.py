@@ -66,6 +66,24 @@ def test_rhs_and_steps_match_reference(vt, path):
     assert s.time == g.meta["time"]
 
 
+@pytest.mark.parametrize("name", ["p3_io10_16x16_pert_rk4", "p1_io10_16x16_pert_rk4", "p2_io6_12x8_pert_fe"])
+@pytest.mark.parametrize("mapping", [0, 1])
+def test_both_warp_mappings_match_reference(vt, name, mapping):
+    """The stage kernel's two warp mappings (one thread per component, or per
+    component pair and node half) compute the same steps to the 1e-12 bar."""
+    g = golden(name)
+    s = vt.Solver(problem_for(vt, g))
+    s.stage_mapping = mapping
+    assert s.stage_mapping == mapping
+    dt, n = g.meta["dt"], g.meta["steps"]
+    if g.meta["stepping"] == 1:
+        s.rk4(dt, n)
+    else:
+        s.forward_euler(dt, n)
+    assert rel_err(s.download(), g["U_final"]) < STATE_RTOL_1STEP * max(1, n)
+    s.close()
+
+
 def test_shipped_10000_steps(vt):
     """Config 1: T = 10*sqrt(2), 10000 RK4 steps, compared every 2500 steps."""
     g = golden("c1_p3_io10_rk4_10000")

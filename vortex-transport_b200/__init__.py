@@ -167,7 +167,11 @@ _SIGNATURES = {
     "vt_batch_step_rk4": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "vt_batch_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(vt_error_info)]),
-    "vt_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "vt_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int)]),
+    "vt_batch_set_mapping": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "vt_set_stage_mapping": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "vt_get_stage_mapping": (ctypes.c_int, [ctypes.c_void_p]),
     "vt_batch_set_blocks_per_sm": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "vt_batch_time_groups": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
     "vt_checkpoint_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
@@ -646,6 +650,15 @@ class Solver:
         self._step_status(lib().vt_tangent_rk4(self._h, float(dt), int(nsteps), ins[0], outp, dev))
         return out
 
+    @property
+    def stage_mapping(self) -> int:
+        """Warp mapping of the stage kernel: 0 component per thread, 1 pair per thread."""
+        return int(lib().vt_get_stage_mapping(self._h))
+
+    @stage_mapping.setter
+    def stage_mapping(self, mapping: int) -> None:
+        _check(lib().vt_set_stage_mapping(self._h, int(mapping)))
+
     def profile_stages(self, dt: float, reps: int) -> np.ndarray:
         ms = (ctypes.c_float * 4)()
         self._step_status(lib().vt_profile_rk4_stages(self._h, float(dt), int(reps), ms))
@@ -783,12 +796,14 @@ class Batch:
         _check(lib().vt_batch_adjoint_info(self._h, int(group), ctypes.byref(info)))
         return info.as_dict()
 
-    def autotune(self, trials: int = 3, cache: str | None = None) -> list[int]:
-        """Resident blocks per SM for each group, tuned on the device and cached
-        in `cache` (a JSON file keyed by the batch's makeup and the GPU)."""
+    def autotune(self, trials: int = 3, cache: str | None = None) -> list[tuple[int, int]]:
+        """(resident blocks per SM, warp mapping) for each group, tuned on the
+        device and cached in `cache` (a JSON file keyed by the batch's makeup
+        and the GPU)."""
         import hashlib
         import json
         key = None
+        ng = lib().vt_batch_groups(self._h)
         if cache:
             import torch
             props = torch.cuda.get_device_properties(self.device)
@@ -799,21 +814,23 @@ class Batch:
                     stored = json.load(f).get(key)
             except (OSError, ValueError):
                 stored = None
-            if stored:
-                arr = (ctypes.c_int * len(stored))(*stored)
-                _check(lib().vt_batch_set_blocks_per_sm(self._h, arr))
-                return list(stored)
-        ng = lib().vt_batch_groups(self._h)
-        arr = (ctypes.c_int * ng)()
-        _check(lib().vt_batch_autotune(self._h, int(trials), arr))
-        best = list(arr)
+            if stored and all(isinstance(x, list) and len(x) == 2 for x in stored):
+                bps = (ctypes.c_int * ng)(*[x[0] for x in stored])
+                maps = (ctypes.c_int * ng)(*[x[1] for x in stored])
+                _check(lib().vt_batch_set_mapping(self._h, maps))
+                _check(lib().vt_batch_set_blocks_per_sm(self._h, bps))
+                return [tuple(x) for x in stored]
+        bps = (ctypes.c_int * ng)()
+        maps = (ctypes.c_int * ng)()
+        _check(lib().vt_batch_autotune(self._h, int(trials), bps, maps))
+        best = [(int(bps[g]), int(maps[g])) for g in range(ng)]
         if cache:
             try:
                 with open(cache) as f:
                     data = json.load(f)
             except (OSError, ValueError):
                 data = {}
-            data[key] = best
+            data[key] = [list(x) for x in best]
             os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
             with open(cache, "w") as f:
                 json.dump(data, f, indent=1)

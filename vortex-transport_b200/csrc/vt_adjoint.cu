@@ -426,6 +426,12 @@ int prepare(vt_ctx* c) {
 
 }  // namespace
 
+void adjoint_invalidate_graphs(vt_ctx* c) {
+  if (!c || !c->adj) return;
+  c->adj->fwd_graph.reset();
+  c->adj->bwd_graph.reset();
+}
+
 void adjoint_release(vt_ctx* c) {
   if (!c || !c->adj) return;
   c->adj->fwd_graph.reset();

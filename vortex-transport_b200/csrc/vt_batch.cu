@@ -268,6 +268,7 @@ int ensure_views(vt_batch* b) {
     c->err = G.err;
     c->ops = G.ops;
     c->launch = G.kern.launch;
+    c->map = G.kern.map;
     c->tile_dt = G.tile_dt;
     double* edt = nullptr;
     const cudaError_t ea = cudaMalloc(reinterpret_cast<void**>(&edt), sizeof(double) * static_cast<size_t>(G.K));
@@ -445,7 +446,7 @@ vt_batch* vt_batch_create(const vt_mesh_desc* descs, int n, int device, int* sta
         (e = cudaMemset(G.U, 0, state_bytes)) || (e = cudaMemset(G.A, 0, state_bytes)) ||
         (e = cudaMemset(G.Sa, 0, state_bytes)) || (e = cudaMemset(G.Sb, 0, state_bytes)) ||
         (e = cudaMemset(G.tile_dt, 0, sizeof(double) * tiles.size())) ||
-        (e = vt::launch_build_tile_items(G.tiles, G.nbr, G.items, G.count, G.ntiles, b->stream)) ||
+        (e = vt::launch_build_tile_items(G.tiles, G.nbr, G.items, G.count, G.ntiles, G.nfq, b->stream)) ||
         (e = cudaStreamSynchronize(b->stream))) {
       set(fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_create upload", e)));
       release(b);
@@ -699,12 +700,30 @@ int vt_batch_last_error(const vt_batch* b, int* instance, vt_error_info* out) {
   return VT_OK;
 }
 
-int vt_batch_autotune(vt_batch* b, int trials, int* blocks_per_sm_out) {
+// Times `trials` RK4 steps (after one untimed) of group G alone with its
+// current kernel and grid; the group's state must be saved by the caller.
+static float time_group_steps(vt_batch* b, vt::Group& G, int trials, cudaEvent_t e0, cudaEvent_t e1) {
+  float tot = 0;
+  for (int r = 0; r < trials + 1; ++r) {
+    cudaEventRecord(e0, b->stream);
+    enqueue_group_step(G, b->stream);
+    cudaEventRecord(e1, b->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r) tot += ms;  // the first repetition warms up
+  }
+  return tot;
+}
+
+int vt_batch_autotune(vt_batch* b, int trials, int* blocks_per_sm_out, int* mapping_out) {
   if (!b || trials < 1) return fail(VT_ERR_INVALID, "vt_batch_autotune: bad argument");
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
-  // candidate persistent grids per group: SMs x {1, 2, 3} blocks; the state is
-  // restored afterwards so tuning does not advance the solution
+  // candidates per group: both warp mappings of the stage kernel (one thread
+  // per component, or per component pair and node half) x persistent grids of
+  // SMs x {1 .. resident limit} blocks; the state is restored afterwards so
+  // tuning does not advance the solution
   std::vector<std::vector<double2>> saved;
   for (auto& G : b->groups) {
     const size_t state = 2 * G.Np * static_cast<size_t>(G.Kpad);
@@ -717,35 +736,28 @@ int vt_batch_autotune(vt_batch* b, int trials, int* blocks_per_sm_out) {
   cudaEventCreate(&e1);
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     vt::Group& G = b->groups[gi];
+    vt::StageKernel best_k = G.kern;
     int best_b = 1;
     float best_ms = 1e30f;
-    int limit = 0;
-    G.kern.configure(&limit);
-    for (int bps = 1; bps <= std::max(1, limit); ++bps) {
-      G.max_blocks = b->sms * bps;
-      float tot = 0;
-      for (int r = 0; r < trials + 1; ++r) {
-        cudaEventRecord(e0, b->stream);
-        for (int st = 0; st < 4; ++st) {
-          const vt::StageArgs a = group_args(G, st == 0 ? G.U : (st == 2 ? G.Sb : G.Sa),
-                                             st == 0 ? G.Sa : (st == 1 ? G.Sb : (st == 2 ? G.Sa : G.U)), st,
-                                             st == 0 ? 1.0 / 6 : (st == 3 ? 0.0 : 1.0 / 3),
-                                             st == 0 ? 0.5 : (st == 1 ? 0.5 : (st == 2 ? 1.0 : 1.0 / 6)));
-          G.kern.launch(a, G.ops.data(), G.max_blocks, b->stream);
+    for (int map : {vt::kMapComponent, vt::kMapPair}) {
+      const vt::StageKernel k = vt::select_kernel(G.p, G.nfq, map);
+      int limit = 0;
+      if (k.configure(&limit)) continue;
+      G.kern = k;
+      for (int bps = 1; bps <= std::max(1, limit); ++bps) {
+        G.max_blocks = b->sms * bps;
+        const float ms = time_group_steps(b, G, trials, e0, e1);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_b = bps;
+          best_k = k;
         }
-        cudaEventRecord(e1, b->stream);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (r) tot += ms;  // first repetition warms up
-      }
-      if (tot < best_ms) {
-        best_ms = tot;
-        best_b = bps;
       }
     }
+    G.kern = best_k;
     G.max_blocks = b->sms * best_b;
     if (blocks_per_sm_out) blocks_per_sm_out[gi] = best_b;
+    if (mapping_out) mapping_out[gi] = best_k.map;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -753,6 +765,37 @@ int vt_batch_autotune(vt_batch* b, int trials, int* blocks_per_sm_out) {
     vt::Group& G = b->groups[gi];
     if (cudaMemcpy(G.U, saved[gi].data(), saved[gi].size() * sizeof(double2), cudaMemcpyHostToDevice))
       return fail(VT_ERR_CUDA, "autotune restore");
+  }
+  for (size_t gi = 0; gi < b->views.size(); ++gi) {  // the adjoint's group views step with the chosen kernels
+    vt_ctx* v = b->views[gi];
+    v->launch = b->groups[gi].kern.launch;
+    v->map = b->groups[gi].kern.map;
+    v->max_blocks = b->groups[gi].max_blocks;
+    vt::adjoint_invalidate_graphs(v);
+  }
+  return capture(b);
+}
+
+int vt_batch_set_mapping(vt_batch* b, const int* mapping) {
+  if (!b || !mapping) return fail(VT_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    if (mapping[gi] != vt::kMapComponent && mapping[gi] != vt::kMapPair)
+      return fail(VT_ERR_INVALID, "vt_batch_set_mapping: mapping must be 0 (component) or 1 (pair)");
+    vt::Group& G = b->groups[gi];
+    const vt::StageKernel k = vt::select_kernel(G.p, G.nfq, mapping[gi]);
+    int limit = 0;
+    const cudaError_t e = k.configure(&limit);
+    if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("vt_batch_set_mapping", e));
+    G.kern = k;
+    G.max_blocks = std::min(G.max_blocks, b->sms * std::max(1, limit));
+    if (gi < b->views.size()) {
+      b->views[gi]->launch = k.launch;
+      b->views[gi]->map = k.map;
+      b->views[gi]->max_blocks = G.max_blocks;
+      vt::adjoint_invalidate_graphs(b->views[gi]);
+    }
   }
   return capture(b);
 }

@@ -34,6 +34,7 @@ struct vt_ctx {
   std::vector<double> ops;
   std::vector<double> minv_ref;  // Np x Np, for the projected initial condition
   vt::LaunchFn launch = nullptr;
+  int map = vt::kDefaultMap;  // warp mapping of the stage kernel
   double time = 0.0;
   cudaGraphExec_t rk4_graph = nullptr;
   double rk4_graph_dt = 0.0;
@@ -73,5 +74,7 @@ cudaError_t soa_to_aos(vt_ctx* c, const double2* src, double* dst);
 
 // Frees the adjoint's buffers (no-op without them).
 void adjoint_release(vt_ctx* c);
+// Drops the adjoint's captured sweep graphs (after the stage kernel changed).
+void adjoint_invalidate_graphs(vt_ctx* c);
 
 }  // namespace vt

@@ -89,6 +89,10 @@ constexpr int kMaxItems = 3 * kTileElems;
 
 enum : int { kStageEuler = 4, kStageRhs = 5 };
 
+// Warp mappings of the stage kernel (vt_tile.cuh): one thread per (element,
+// component), or per (element, component pair, node half).
+enum : int { kMapComponent = 0, kMapPair = 1 };
+
 // First-error key: (stage epoch << 40) | (((e * nfq + q) * 3 + s) * 4 + code).
 // The minimum over all failures is the failure the reference's serial loop
 // meets first: earliest stage, then element, face point, side, check.

@@ -19,10 +19,18 @@ struct StageKernel {
   // Sets the dynamic shared-memory attribute on the current device and
   // reports resident blocks per SM. Call before any launch or capture.
   ConfigFn configure = nullptr;
+  // Warp mapping of the instantiation (kMapComponent or kMapPair, vt_tile.cuh).
+  int map = 0;
 };
 
-// Empty (null members) for p outside 0..3 or nfq outside 1..10.
-StageKernel select_kernel(int p, int nfq);
+// The mapping a context uses unless told otherwise (the pair mapping: 8% faster
+// at p = 3 on the 768 x 768 mesh).
+constexpr int kDefaultMap = kMapPair;
+
+// Empty (null members) for p outside 0..3, nfq outside 1..10.
+StageKernel select_kernel(int p, int nfq, int map = kDefaultMap);
+StageKernel select_kernel_component(int p, int nfq);
+StageKernel select_kernel_pair(int p, int nfq);
 
 // Number of doubles of the StageOps<P, NFQ> block for (p, nfq).
 int stage_ops_doubles(int p, int nfq);
@@ -43,7 +51,8 @@ std::vector<int4> grid_tile_runs(int nx, int ny);
 
 // Device-side: tiles of 64 consecutive elements, then the per-tile face lists.
 cudaError_t launch_contiguous_tiles(int4* tiles, int K, int ntiles, cudaStream_t st);
-cudaError_t launch_build_tile_items(const int4* tiles, const int4* nbr, int* items, int* count, int ntiles,
+// nfq decides where the face items that read global memory are placed (vt_schedule.cuh).
+cudaError_t launch_build_tile_items(const int4* tiles, const int4* nbr, int* items, int* count, int ntiles, int nfq,
                                     cudaStream_t st);
 
 }  // namespace vt

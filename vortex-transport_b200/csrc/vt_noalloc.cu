@@ -202,7 +202,7 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
     return fail(VT_ERR_CUDA, std::string("scratch reset: ") + cudaGetErrorString(e));
   vt::pack_geometry_kernel<<<(K + 255) / 256, 256, 0, st>>>(*m, geo, nbr, cv.Kpad, errw);
   if ((e = vt::launch_contiguous_tiles(tiles, K, cv.ntiles, st)) ||
-      (e = vt::launch_build_tile_items(tiles, nbr, items, count, cv.ntiles, st)))
+      (e = vt::launch_build_tile_items(tiles, nbr, items, count, cv.ntiles, m->n_line_points, st)))
     return fail(VT_ERR_CUDA, std::string("tile schedule: ") + cudaGetErrorString(e));
   const long long nrow = static_cast<long long>(K) * 2 * Np;
   const int tb = static_cast<int>((nrow + 255) / 256);

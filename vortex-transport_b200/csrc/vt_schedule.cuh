@@ -64,8 +64,15 @@ __global__ void contiguous_tiles_kernel(int4* tiles, int K, int ntiles) {
 // the tile, a side-0 neighbour staged in shared memory, any other neighbour
 // read from global memory -- so that a warp's work items take one path, and
 // in (element, side) order within a group.
+//
+// The stage kernel gives work item w = item * nfq + q to thread w mod 256, so
+// with nw = n * nfq > 256 the threads below L = nw mod 256 (or all, when L is
+// 0) take one item more than the rest. The items of the last group wait on
+// global loads; they are placed on threads with one item fewer (item indices
+// from ceil(L / nfq) on, in the first round) when they fit there, so that
+// their latency does not lengthen the face phase.
 __global__ void build_tile_items_kernel(const int4* __restrict__ tiles, const int4* __restrict__ nbr,
-                                        int* __restrict__ items, int* __restrict__ count) {
+                                        int* __restrict__ items, int* __restrict__ count, int nfq) {
   __shared__ int warp_n[3][8];
   const int tile = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int4 run = tiles[tile];
@@ -94,18 +101,26 @@ __global__ void build_tile_items_kernel(const int4* __restrict__ tiles, const in
     if (lane == 0) warp_n[k][warp] = __popc(m[k]);
   }
   __syncthreads();
-  int base = 0;
-  for (int k = 0; k < cls; ++k)
-    for (int w = 0; w < 8; ++w) base += warp_n[k][w];
-  for (int w = 0; w < warp; ++w) base += warp_n[cls][w];
-  if (take)
-    items[static_cast<long long>(tile) * kMaxItems + base + __popc(m[cls] & ((1u << lane) - 1u))] = code;
-  if (t == 0) {
-    int n = 0;
-    for (int k = 0; k < 3; ++k)
-      for (int w = 0; w < 8; ++w) n += warp_n[k][w];
-    count[tile] = n;
+  int n_cls[3] = {0, 0, 0};
+  for (int k = 0; k < 3; ++k)
+    for (int w = 0; w < 8; ++w) n_cls[k] += warp_n[k][w];
+  const int n = n_cls[0] + n_cls[1] + n_cls[2];
+  // where the global-gather group goes: item index k0, or after the others
+  const int T = 4 * kTileElems, nw = n * nfq;
+  const int L = nw % T;
+  const int k0 = nfq > 0 ? (L + nfq - 1) / nfq : 0;
+  const bool move = nw > T && L > 0 && (k0 + n_cls[2]) * nfq <= T && k0 <= n_cls[0] + n_cls[1];
+  int rank = 0;  // position within the (class 0, class 1, class 2) order
+  for (int k = 0; k < cls; ++k) rank += n_cls[k];
+  for (int w = 0; w < warp; ++w) rank += warp_n[cls][w];
+  rank += __popc(m[cls] & ((1u << lane) - 1u));
+  int slot = rank;
+  if (move) {
+    if (cls == 2) slot = k0 + (rank - n_cls[0] - n_cls[1]);
+    else if (rank >= k0) slot = rank + n_cls[2];
   }
+  if (take) items[static_cast<long long>(tile) * kMaxItems + slot] = code;
+  if (t == 0) count[tile] = n;
 }
 
 }  // namespace vt

@@ -523,7 +523,7 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
       e = vt::launch_contiguous_tiles(c->tiles, K, c->ntiles, c->stream);
     else
       e = cudaMemcpyAsync(c->tiles, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice, c->stream);
-    if (!e) e = vt::launch_build_tile_items(c->tiles, c->nbr, c->tile_items, c->tile_count, c->ntiles, c->stream);
+    if (!e) e = vt::launch_build_tile_items(c->tiles, c->nbr, c->tile_items, c->tile_count, c->ntiles, c->nfq, c->stream);
     if (!e) e = cudaStreamSynchronize(c->stream);
     if (e) {
       set(fail(VT_ERR_CUDA, vt::cuda_msg("tile schedule", e)));
@@ -679,7 +679,7 @@ vt_ctx* vt_create_structured(const vt_params* prm, const vt_vortex* ic_in, int d
     else
       e = cudaMemcpyAsync(c->tiles, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice, c->stream);
   }
-  if (!e) e = vt::launch_build_tile_items(c->tiles, c->nbr, c->tile_items, c->tile_count, c->ntiles, c->stream);
+  if (!e) e = vt::launch_build_tile_items(c->tiles, c->nbr, c->tile_items, c->tile_count, c->ntiles, c->nfq, c->stream);
   if (!e) e = cudaStreamSynchronize(c->stream);
   cudaFree(verts);
   if (dtab) cudaFree(dtab);
@@ -962,6 +962,29 @@ int vt_load_state(vt_ctx* c, const char* path) {
 }
 
 void* vt_stream(vt_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int vt_set_stage_mapping(vt_ctx* c, int mapping) {
+  if (!c || (mapping != vt::kMapComponent && mapping != vt::kMapPair))
+    return fail(VT_ERR_INVALID, "vt_set_stage_mapping: mapping must be 0 (component) or 1 (pair)");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const vt::StageKernel sk = vt::select_kernel(c->p, c->nfq, mapping);
+  int per_sm = 0, sms = 0;
+  cudaError_t e = sk.configure(&per_sm);
+  if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("vt_set_stage_mapping", e));
+  c->launch = sk.launch;
+  c->map = mapping;
+  c->max_blocks = sms * (per_sm > 0 ? per_sm : 1);
+  if (c->rk4_graph) {  // the captured step holds the old kernel
+    cudaGraphExecDestroy(c->rk4_graph);
+    c->rk4_graph = nullptr;
+  }
+  vt::adjoint_invalidate_graphs(c);
+  return VT_OK;
+}
+
+int vt_get_stage_mapping(const vt_ctx* c) { return c ? c->map : -1; }
 
 int vt_test_bulk_wait(vt_ctx* c, unsigned tries, int issue_no_copies) {
   if (!c) return fail(VT_ERR_INVALID, "vt_test_bulk_wait: null context");

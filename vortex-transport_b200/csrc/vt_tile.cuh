@@ -156,7 +156,140 @@ __device__ __forceinline__ void run_sync(int t) {
   else asm volatile("bar.sync 1, 128;" ::: "memory");
 }
 
-template <int P, int NFQ>
+// ---- warp mappings -------------------------------------------------------------------
+// Thread t of a block holds element column el = t % 64 and group g = t / 64
+// (uniform per warp; warps of equal parity hold one run). Two mappings of the
+// work onto (el, g), chosen per order p (StageKernel, vt_launch.cu):
+//   component (kMapComponent): g is the conserved component c; the thread
+//     forms every face point's trace and every node's update of component c;
+//   pair (kMapPair): g = (half, h) with h the component pair of the HBM
+//     layout ((rho, rho u) or (rho v, rho E)); the thread forms both
+//     components of pair h for half of the face points (traces) and half of
+//     the nodes (lift, volume, update): [0, QH) / [0, NH) or the rest, with
+//     QH = ceil(nfq / 2), NH = ceil(Np / 2). Shared- and global-memory
+//     accesses are then 16 bytes wide (half the load/store instructions) for
+//     the same floating-point work.
+// The face buffer holds the same bytes either way: [s][c][q][el] doubles for
+// the component mapping, [s][q][h][el] double2 for the pair mapping (and the
+// nodal flux [j][8][el] doubles or [j][4][el] double2).
+template <int P, int NFQ, int HALF>
+__device__ __forceinline__ void pair_traces(const StageOps<P, NFQ>& ops, const double2* S, double2* FB2, int h,
+                                            int el) {
+  constexpr int NP = np_of_p(P), NE = P + 1, ES = kTileElems + 1, QH = (NFQ + 1) / 2;
+  constexpr int q0 = HALF * QH, q1 = (HALF + 1) * QH < NFQ ? (HALF + 1) * QH : NFQ;
+  double2 u[NP];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) u[i] = S[(2 * i + h) * ES + el];
+#pragma unroll
+  for (int s = 0; s < 3; ++s)
+#pragma unroll
+    for (int q = q0; q < q1; ++q) {
+      double vx = 0.0, vy = 0.0;
+#pragma unroll
+      for (int k = 0; k < NE; ++k) {
+        vx = fma(ops.tp[s][q][k], u[edge_node(P, s, k)].x, vx);
+        vy = fma(ops.tp[s][q][k], u[edge_node(P, s, k)].y, vy);
+      }
+      FB2[((s * NFQ + q) * 2 + h) * ES + el] = make_double2(vx, vy);
+    }
+}
+
+template <int P, int NFQ, int HALF>
+__device__ __forceinline__ void pair_lift(const StageOps<P, NFQ>& ops, const double2* FB2, int h, int el,
+                                          double2 lsa, double2 lsb, double2* r) {
+  constexpr int NP = np_of_p(P), ES = kTileElems + 1, NH = (NP + 1) / 2, base = HALF * NH;
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const double ls = s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x);
+#pragma unroll
+    for (int q = 0; q < NFQ; ++q) {
+      const double2 f = FB2[((s * NFQ + q) * 2 + h) * ES + el];
+      const double fx = ls * f.x, fy = ls * f.y;
+#pragma unroll
+      for (int i = 0; i < NH; ++i)
+        if (base + i < NP) {
+          r[i].x = fma(-ops.lift[s][base + i][q], fx, r[i].x);
+          r[i].y = fma(-ops.lift[s][base + i][q], fy, r[i].y);
+        }
+    }
+  }
+}
+
+template <int P, int NFQ, int HALF>
+__device__ __forceinline__ void pair_volume(const StageOps<P, NFQ>& ops, const double2* G2, int h, int el,
+                                            double2* r) {
+  constexpr int NP = np_of_p(P), ES = kTileElems + 1, NH = (NP + 1) / 2, base = HALF * NH;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const double2 gx = G2[(j * 4 + h) * ES + el];
+    const double2 gy = G2[(j * 4 + 2 + h) * ES + el];
+#pragma unroll
+    for (int i = 0; i < NH; ++i)
+      if (base + i < NP) {
+        r[i].x = fma(ops.D[0][base + i][j], gx.x, fma(ops.D[1][base + i][j], gy.x, r[i].x));
+        r[i].y = fma(ops.D[0][base + i][j], gx.y, fma(ops.D[1][base + i][j], gy.y, r[i].y));
+      }
+  }
+}
+
+// Non-coherent loads issued where they are written, so that the stage
+// update's first operand is in flight during the volume phase (the compiler
+// would otherwise sink them to their use).
+__device__ __forceinline__ double ld_early(const double* p) {
+  double v;
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double2 ld_early2(const double2* p) {
+  double2 v;
+  asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+
+// The stage's read-only operand that the update needs besides the
+// accumulator: U_n (stage 0, forward Euler), the accumulator (stage 3) or
+// the base U_n (stages 1, 2); none for the bare right-hand side.
+__device__ __forceinline__ const double2* first_operand(const StageArgs& a) {
+  return (a.stage == 0 || a.stage == kStageEuler) ? a.in : (a.stage == 3 ? a.acc : a.base);
+}
+
+__device__ __forceinline__ double2 fma2(double c, double2 r, double2 u) {
+  return make_double2(fma(c, r.x, u.x), fma(c, r.y, u.y));
+}
+
+// Stage update of pair h of this half's nodes; pre holds first_operand's values.
+template <int P, int HALF>
+__device__ __forceinline__ void pair_update(const StageArgs& a, int e, int h, double c_acc, double c_out,
+                                            const double2* r, const double2* pre) {
+  constexpr int NP = np_of_p(P), NH = (NP + 1) / 2;
+  const long long KP = a.Kpad;
+  const long long o = (2 * HALF * NH + h) * KP + e;  // row 2 * node + h of this half's first node
+#pragma unroll
+  for (int i = 0; i < NH; ++i) {
+    if (HALF * NH + i >= NP) break;
+    const long long x = o + i * 2 * KP;
+    switch (a.stage) {
+      case 0:
+        a.acc[x] = fma2(c_acc, r[i], pre[i]);
+        a.out[x] = fma2(c_out, r[i], pre[i]);
+        break;
+      case 1:
+      case 2:
+        a.acc[x] = fma2(c_acc, r[i], a.acc[x]);
+        a.out[x] = fma2(c_out, r[i], pre[i]);
+        break;
+      case 3:
+      case kStageEuler:
+        a.out[x] = fma2(c_out, r[i], pre[i]);
+        break;
+      default:
+        a.out[x] = r[i];
+        break;
+    }
+  }
+}
+
+template <int P, int NFQ, int MAP>
 // Three 256-thread blocks per SM (<= 80 registers per thread) keep 24 warps
 // resident alongside 3 x ~75 KB of shared memory.
 __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const StageArgs a,
@@ -167,10 +300,12 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   constexpr int NE = L::NE;
   constexpr int ES = L::ES;
   constexpr int T = 4 * E;
+  constexpr bool PAIR = MAP == kMapPair;
   extern __shared__ __align__(16) unsigned char smem[];
   double2* S = reinterpret_cast<double2*>(smem + L::kS);
   double2* H = reinterpret_cast<double2*>(smem + L::kH);
   double* FB = reinterpret_cast<double*>(smem + L::kFB);
+  double2* FB2 = reinterpret_cast<double2*>(smem + L::kFB);
   double* TM = reinterpret_cast<double*>(smem + L::kTM);
   int4* NB = reinterpret_cast<int4*>(smem + L::kNB);
   int* EL = reinterpret_cast<int*>(smem + L::kEL);
@@ -179,7 +314,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   int* abort_flag = reinterpret_cast<int*>(smem + L::kBar + 8);
 
   const int t = threadIdx.x;
-  const int col = t % E, grp = t / E;  // load mapping; also (element, component) later
+  const int col = t % E, grp = t / E;  // load mapping; also (element, group) later
   const int lane = t & 31;
   const long long KP = a.Kpad;
   const int G = gridDim.x;
@@ -201,7 +336,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   if (tile >= a.ntiles) return;
   int4 run = __ldg(a.tiles + tile);
   int nitems = __ldg(a.tile_count + tile);
-  int my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
+  int my_item = t < kMaxItems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
   int4 my_nb = make_int4(0, 0, 0, 0);
   double2 hreg[2];
   {
@@ -221,21 +356,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   for (; tile < a.ntiles; tile += G) {
     const bool has_next = tile + G < a.ntiles;
 
-    // ---- prefetch: the next tile into L2 (its state copies start in phase 5), this
-    // tile's RK rows into L2 and its geometry rows into L1 -----------------------
-    if (t < 64) {
-      if (has_next) {
-        const int4 rr = __ldg(a.tiles + tile + G);
-        const int which = t & 1, r = t >> 1;
-        const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
-        if (len > 0) {
-          const unsigned bytes = static_cast<unsigned>(len) * 16u;
-          if (r < 2 * NP) prefetch_l2(a.in + r * KP + start, bytes);
-          else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
-          else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
-        }
-      }
-    } else if (t < 64 + 8 * NP) {
+    // ---- prefetch: this tile's RK operand rows into L2 (read in phase 6) and its
+    // geometry rows into L1. The next tile's state is not prefetched: its bulk
+    // copies, issued in phase 5, read it from HBM themselves (prefetching it
+    // as well was 1.6% slower) -------------------------------------------------
+    if (t >= 64 && t < 64 + 8 * NP) {
       const int l = t - 64, which = l & 1, r = l >> 1;
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
       if (len > 0) {
@@ -246,7 +371,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
           prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
         }
       }
-    } else if (t < 64 + 8 * NP + 56) {
+    } else if (t >= 64 + 8 * NP && t < 64 + 8 * NP + 56) {
       // this tile's 7 geometry rows into L1 (4 lines per 32-element run)
       const int l = t - 64 - 8 * NP, row = l >> 3, which = (l >> 2) & 1, line = l & 3;
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
@@ -281,8 +406,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     }
     parity ^= 1u;
 
-    // ---- 2. own traces: Tr[s][c][q][el], thread (element el, component c) ----------
-    {
+    // ---- 2. own traces at every face point -------------------------------------------
+    if constexpr (PAIR) {
+      if (grp >> 1) pair_traces<P, NFQ, 1>(ops, S, FB2, grp & 1, col);
+      else pair_traces<P, NFQ, 0>(ops, S, FB2, grp & 1, col);
+    } else {
       const int cc = grp, el = col;
       const double* Sd = reinterpret_cast<const double*>(S);
       double u[NP];
@@ -312,11 +440,21 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       const int e = EL[el];
       const double2 n = __ldg(a.geo + (2 + s) * KP + e);
       double up[4], um[4];
+      if constexpr (PAIR) {
+        const double2 x0 = FB2[((s * NFQ + q) * 2) * ES + el], x1 = FB2[((s * NFQ + q) * 2 + 1) * ES + el];
+        up[0] = x0.x, up[1] = x0.y, up[2] = x1.x, up[3] = x1.y;
+      } else {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) up[c] = FB[((s * 4 + c) * NFQ + q) * ES + el];
+        for (int c = 0; c < 4; ++c) up[c] = FB[((s * 4 + c) * NFQ + q) * ES + el];
+      }
       if (mirror) {
+        if constexpr (PAIR) {
+          const double2 y0 = FB2[((s * NFQ + qm) * 2) * ES + nl], y1 = FB2[((s * NFQ + qm) * 2 + 1) * ES + nl];
+          um[0] = y0.x, um[1] = y0.y, um[2] = y1.x, um[3] = y1.y;
+        } else {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) um[c] = FB[((s * 4 + c) * NFQ + qm) * ES + nl];
+          for (int c = 0; c < 4; ++c) um[c] = FB[((s * 4 + c) * NFQ + qm) * ES + nl];
+        }
       } else {
         const int4 nb4 = NB[el];
         const int nb = s == 0 ? nb4.x : (s == 1 ? nb4.y : nb4.z);
@@ -343,64 +481,91 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       double f[4];
       const int code = roe_flux(up, um, n.x, n.y, f);
       if (code) record_error(a, NFQ, e, q, s, code);
+      if constexpr (PAIR) {
+        FB2[((s * NFQ + q) * 2) * ES + el] = make_double2(f[0], f[1]);
+        FB2[((s * NFQ + q) * 2 + 1) * ES + el] = make_double2(f[2], f[3]);
+        if (mirror) {
+          FB2[((s * NFQ + qm) * 2) * ES + nl] = make_double2(-f[0], -f[1]);
+          FB2[((s * NFQ + qm) * 2 + 1) * ES + nl] = make_double2(-f[2], -f[3]);
+        }
+      } else {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + q) * ES + el] = f[c];
-      if (mirror) {
+        for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + q) * ES + el] = f[c];
+        if (mirror) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + qm) * ES + nl] = -f[c];
+          for (int c = 0; c < 4; ++c) FB[((s * 4 + c) * NFQ + qm) * ES + nl] = -f[c];
+        }
       }
     }
     __syncthreads();
 
-    // next tile's metadata (next_run has arrived by now)
+    // next tile's metadata (next_run has arrived by now); the item rows are
+    // kMaxItems wide, so the load need not wait for the item count
     if (has_next) {
       nitems = __ldg(a.tile_count + tile + G);
-      my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
+      my_item = t < kMaxItems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       my_nb = pos < (second ? next_run.w : next_run.y) ? __ldg(a.nbr + (second ? next_run.z : next_run.x) + pos)
                                                        : make_int4(0, 0, 0, 0);
     }
 
-    // ---- 4. lift: thread (element el, component c) --------------------------------------
-    const int c = grp;  // uniform per warp
+    // ---- 4. lift ---------------------------------------------------------------------------
     const int el = col;
     const int e = EL[el];
     const bool valid = e >= 0;
     const int eg = valid ? e : run.x;
-    double r[NP];
-#pragma unroll
-    for (int i = 0; i < NP; ++i) r[i] = 0.0;
+    constexpr int NH = (NP + 1) / 2;
+    constexpr int NR = PAIR ? NH : NP;  // accumulators: double2 per node pair, or one double per node
+    double2 r2[PAIR ? NH : 1];
+    double r[PAIR ? 1 : NP];
     {
       const double2 lsa = __ldg(a.geo + 5 * KP + eg);
       const double2 lsb = __ldg(a.geo + 6 * KP + eg);
+      if constexpr (PAIR) {
 #pragma unroll
-      for (int s = 0; s < 3; ++s) {
-        const double ls = s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x);
+        for (int i = 0; i < NH; ++i) r2[i] = make_double2(0.0, 0.0);
+        if (grp >> 1) pair_lift<P, NFQ, 1>(ops, FB2, grp & 1, el, lsa, lsb, r2);
+        else pair_lift<P, NFQ, 0>(ops, FB2, grp & 1, el, lsa, lsb, r2);
+      } else {
+        const int c = grp;
 #pragma unroll
-        for (int q = 0; q < NFQ; ++q) {
-          const double fs = ls * FB[((s * 4 + c) * NFQ + q) * ES + el];
+        for (int i = 0; i < NP; ++i) r[i] = 0.0;
 #pragma unroll
-          for (int i = 0; i < NP; ++i) r[i] = fma(-ops.lift[s][i][q], fs, r[i]);
+        for (int s = 0; s < 3; ++s) {
+          const double ls = s == 0 ? lsa.x : (s == 1 ? lsa.y : lsb.x);
+#pragma unroll
+          for (int q = 0; q < NFQ; ++q) {
+            const double fs = ls * FB[((s * 4 + c) * NFQ + q) * ES + el];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) r[i] = fma(-ops.lift[s][i][q], fs, r[i]);
+          }
         }
       }
     }
+    (void)NR;
     run_sync(t);
 
-    // ---- 5. nodal flux of every node, once: G[j][0..3] xi, G[j][4..7] eta ---------------
-    double* Gs = FB;
+    // ---- 5. nodal flux of every node, once, contracted with the inverse Jacobian --------
     if (P > 0) {
       const double2 j0 = __ldg(a.geo + 0 * KP + eg);
       const double2 j1 = __ldg(a.geo + 1 * KP + eg);
-      for (int j = c; j < NP; j += 4) {
+      for (int j = grp; j < NP; j += 4) {
         const double2 s0 = S[(2 * j) * ES + el], s1 = S[(2 * j + 1) * ES + el];
         const double sv[4] = {s0.x, s0.y, s1.x, s1.y};
         double gxi[4], geta[4];
         contravariant_flux(sv, j0.x, j0.y, j1.x, j1.y, gxi, geta);
+        if constexpr (PAIR) {  // G2[j][0..1] xi pairs, G2[j][2..3] eta pairs
+          FB2[(j * 4 + 0) * ES + el] = make_double2(gxi[0], gxi[1]);
+          FB2[(j * 4 + 1) * ES + el] = make_double2(gxi[2], gxi[3]);
+          FB2[(j * 4 + 2) * ES + el] = make_double2(geta[0], geta[1]);
+          FB2[(j * 4 + 3) * ES + el] = make_double2(geta[2], geta[3]);
+        } else {  // G[j][0..3] xi, G[j][4..7] eta
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          Gs[(j * 8 + cc) * ES + el] = gxi[cc];
-          Gs[(j * 8 + 4 + cc) * ES + el] = geta[cc];
+          for (int cc = 0; cc < 4; ++cc) {
+            FB[(j * 8 + cc) * ES + el] = gxi[cc];
+            FB[(j * 8 + 4 + cc) * ES + el] = geta[cc];
+          }
         }
       }
     }
@@ -419,63 +584,87 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       }
     }
 
-    // ---- 6a. volume ------------------------------------------------------------------
+    // the stage update's first operand, requested now so that it is in flight
+    // during the volume phase
+    const bool upd = valid && a.stage != kStageRhs;
+    const double2* src = first_operand(a);
+    double2 pre2[PAIR ? NH : 1];
+    double pre[PAIR ? 1 : NP];
+    if constexpr (PAIR) {
+      const int h = grp & 1, half = grp >> 1;
+      const long long o = (2 * half * NH + h) * KP + eg;
+#pragma unroll
+      for (int i = 0; i < NH; ++i)
+        pre2[i] = upd && half * NH + i < NP ? ld_early2(src + o + i * 2 * KP) : make_double2(0.0, 0.0);
+    } else {
+      const int c = grp;
+      const double* s1 = reinterpret_cast<const double*>(src) + ((c >> 1) * KP + eg) * 2 + (c & 1);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) pre[i] = upd ? ld_early(s1 + i * 4 * KP) : 0.0;
+    }
+
+    // ---- 6a. volume D_xi G_xi + D_eta G_eta --------------------------------------------
     if (P > 0) {
+      if constexpr (PAIR) {
+        if (grp >> 1) pair_volume<P, NFQ, 1>(ops, FB2, grp & 1, el, r2);
+        else pair_volume<P, NFQ, 0>(ops, FB2, grp & 1, el, r2);
+      } else {
+        const int c = grp;
 #pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const double gx = Gs[(j * 8 + c) * ES + el];
-        const double gy = Gs[(j * 8 + 4 + c) * ES + el];
+        for (int j = 0; j < NP; ++j) {
+          const double gx = FB[(j * 8 + c) * ES + el];
+          const double gy = FB[(j * 8 + 4 + c) * ES + el];
 #pragma unroll
-        for (int i = 0; i < NP; ++i) r[i] = fma(ops.D[0][i][j], gx, fma(ops.D[1][i][j], gy, r[i]));
+          for (int i = 0; i < NP; ++i) r[i] = fma(ops.D[0][i][j], gx, fma(ops.D[1][i][j], gy, r[i]));
+        }
       }
     }
 
-    // ---- 6b. stage update: component c of every node ----------------------------------
+    // ---- 6b. stage update ------------------------------------------------------------------
     if (valid) {
       const double dtt = a.tile_dt ? __ldg(a.tile_dt + tile) : 1.0;
       const double c_acc = a.c_acc * dtt, c_out = a.c_out * dtt;
-      const int h = c >> 1, part = c & 1;
-      const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
-      const double* in = reinterpret_cast<const double*>(a.in) + off0;
-      const double* base = reinterpret_cast<const double*>(a.base) + off0;
-      double* acc = reinterpret_cast<double*>(a.acc) + off0;
-      double* out = reinterpret_cast<double*>(a.out) + off0;
-      const long long step = 4 * KP;  // doubles between node rows of the same pair
-      switch (a.stage) {
-        case 0:
+      if constexpr (PAIR) {
+        if (grp >> 1) pair_update<P, 1>(a, e, grp & 1, c_acc, c_out, r2, pre2);
+        else pair_update<P, 0>(a, e, grp & 1, c_acc, c_out, r2, pre2);
+      } else {
+        const int c = grp, h = c >> 1, part = c & 1;
+        const long long off0 = (h * KP + e) * 2 + part;  // node 0; node i adds i * 4 * KP
+        double* acc = reinterpret_cast<double*>(a.acc) + off0;
+        double* out = reinterpret_cast<double*>(a.out) + off0;
+        const long long step = 4 * KP;  // doubles between node rows of the same pair
+        switch (a.stage) {
+          case 0:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            const double u = __ldg(in + i * step);
-            acc[i * step] = fma(c_acc, r[i], u);
-            out[i * step] = fma(c_out, r[i], u);
-          }
-          break;
-        case 1:
-        case 2:
+            for (int i = 0; i < NP; ++i) {
+              acc[i * step] = fma(c_acc, r[i], pre[i]);
+              out[i * step] = fma(c_out, r[i], pre[i]);
+            }
+            break;
+          case 1:
+          case 2:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            acc[i * step] = fma(c_acc, r[i], acc[i * step]);
-            out[i * step] = fma(c_out, r[i], __ldg(base + i * step));
-          }
-          break;
-        case 3:
+            for (int i = 0; i < NP; ++i) {
+              acc[i * step] = fma(c_acc, r[i], acc[i * step]);
+              out[i * step] = fma(c_out, r[i], pre[i]);
+            }
+            break;
+          case 3:
+          case kStageEuler:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], acc[i * step]);
-          break;
-        case kStageEuler:
+            for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], pre[i]);
+            break;
+          default:
 #pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], __ldg(in + i * step));
-          break;
-        default:
-#pragma unroll
-          for (int i = 0; i < NP; ++i) out[i * step] = r[i];
-          break;
+            for (int i = 0; i < NP; ++i) out[i * step] = r[i];
+            break;
+        }
       }
     }
     run = next_run;
-    // the four warps of a run hold different components of the same elements:
-    // none may start the next tile's traces (which reuse rows of the face /
-    // flux buffer) before the others are done with this tile's
+    // the four warps of a run work on the same elements: none may start the
+    // next tile's traces (which reuse rows of the face / flux buffer) before
+    // the others are done with this tile's volume phase
     run_sync(t);
   }
 
