@@ -385,7 +385,7 @@ vt_batch* vt_batch_create(const vt_mesh_desc* descs, int n, int device, int* sta
   for (auto& G : b->groups) {
     G.kern = vt::select_kernel(G.p, G.nfq);
     int per_sm = 0;
-    if ((e = G.kern.configure(&per_sm))) {
+    if ((e = vt::tensor_maps_available()) || (e = G.kern.configure(&per_sm))) {
       set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
       release(b);
       return nullptr;

@@ -9,6 +9,8 @@
 // bytes; one element's state is 2*Np 16-byte loads.
 #pragma once
 
+#include <cuda.h>
+
 #include <cstdint>
 
 namespace vt {
@@ -79,6 +81,10 @@ struct StageArgs {
   // test_flags issues no state copies at all, so every wait gives up.
   unsigned wait_tries = 0;
   int test_flags = 0;
+  // 2-D tensor maps of in / acc / base, [2 Np rows] x [2 Kpad doubles], box of
+  // 2 Np rows x 64 doubles (one 32-element run); encoded on the host by the
+  // launcher, read by the tensor copies through this grid-constant parameter
+  CUtensorMap map_in, map_acc, map_base;
 };
 
 enum : int { kTestNoCopies = 1 };

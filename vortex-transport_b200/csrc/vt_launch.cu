@@ -1,12 +1,51 @@
 // Kernel selection by (p, nfq, warp mapping) -- the instantiations are in
 // vt_stage_component.cu and vt_stage_pair.cu -- and the tile schedule kernels
 // (vt_launch.h).
+#include <cuda.h>
+
 #include <cstring>
+#include <mutex>
 
 #include "vt_launch.h"
 #include "vt_schedule.cuh"
 
 namespace vt {
+
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+}  // namespace
+
+cudaError_t tensor_maps_available() { return encode_tiled() ? cudaSuccess : cudaErrorNotSupported; }
+
+cudaError_t encode_state_map(CUtensorMap* m, const void* base, long long Kpad, int Np) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn) return cudaErrorNotSupported;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(2 * Kpad), static_cast<cuuint64_t>(2 * Np)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(2 * Kpad * sizeof(double))};
+  const cuuint32_t box[2] = {2 * kTileRun, static_cast<cuuint32_t>(2 * Np)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
 
 StageKernel select_kernel(int p, int nfq, int map) {
   return map == kMapPair ? select_kernel_pair(p, nfq) : select_kernel_component(p, nfq);

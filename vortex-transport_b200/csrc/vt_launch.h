@@ -49,6 +49,15 @@ std::vector<int4> structured_tile_runs(int K, const int32_t* type, const int32_t
 // The same runs from the grid size alone (empty unless nx, ny suit them).
 std::vector<int4> grid_tile_runs(int nx, int ny);
 
+// Encodes the 2-D tensor map of a state vector for the stage kernel's tensor
+// copies: [2 Np rows] x [2 Kpad doubles], box of 2 Np rows x 64 doubles (one
+// run of 32 elements). Host only; a pure encoding (cuTensorMapEncodeTiled,
+// reached through the runtime's driver entry point), no allocation.
+cudaError_t encode_state_map(CUtensorMap* map, const void* base, long long Kpad, int Np);
+// cudaSuccess when the driver provides the tensor-map encoder (looked up once;
+// call before any stream capture).
+cudaError_t tensor_maps_available();
+
 // Device-side: tiles of 64 consecutive elements, then the per-tile face lists.
 cudaError_t launch_contiguous_tiles(int4* tiles, int K, int ntiles, cudaStream_t st);
 // nfq decides where the face items that read global memory are placed (vt_schedule.cuh).

@@ -175,7 +175,8 @@ int vt_step_rk4_noalloc(const vt_device_mesh* m, const double* dU_in, double* dU
   if (e || !scratch_ptr)
     return fail(VT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   int per_sm = 0;
-  if ((e = pk.configure(&per_sm))) return fail(VT_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
+  if ((e = vt::tensor_maps_available()) || (e = pk.configure(&per_sm)))
+    return fail(VT_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
   const int max_blocks = ds->sms * (per_sm > 0 ? per_sm : 1);
 
   unsigned char* base = static_cast<unsigned char*>(scratch_ptr);

@@ -446,7 +446,8 @@ vt_ctx* vt_create(const vt_mesh_desc* d, int device, int* status) {
   const vt::StageKernel sk = vt::select_kernel(c->p, c->nfq);
   c->launch = sk.launch;
   int per_sm = 0, sms = 0;
-  if ((e = sk.configure(&per_sm)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device))) {
+  if ((e = vt::tensor_maps_available()) || (e = sk.configure(&per_sm)) ||
+      (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device))) {
     set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
     delete c;
     return nullptr;
@@ -594,7 +595,8 @@ vt_ctx* vt_create_structured(const vt_params* prm, const vt_vortex* ic_in, int d
   const vt::StageKernel sk = vt::select_kernel(p, nfq);
   c->launch = sk.launch;
   int per_sm = 0, sms = 0;
-  if ((e = sk.configure(&per_sm)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device))) {
+  if ((e = vt::tensor_maps_available()) || (e = sk.configure(&per_sm)) ||
+      (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device))) {
     set(fail(VT_ERR_CUDA, vt::cuda_msg("stage kernel attributes", e)));
     delete c;
     return nullptr;

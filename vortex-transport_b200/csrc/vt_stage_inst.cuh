@@ -30,7 +30,14 @@ cudaError_t launch_stage(const StageArgs& a, const double* ops, int max_blocks, 
   static_assert(sizeof(StageOps<P, NFQ>) % sizeof(double) == 0, "operator block is doubles");
   std::memcpy(&o, ops, sizeof(o));
   const int grid = a.ntiles < max_blocks ? a.ntiles : max_blocks;
-  tile_stage_kernel<P, NFQ, MAP><<<grid, 4 * kTileElems, Lay::kBytes, st>>>(a, o);
+  // the tensor maps of this launch's state vectors (host-side encoding, no allocation)
+  StageArgs k = a;
+  constexpr int NP = np_of_p(P);
+  cudaError_t e = encode_state_map(&k.map_in, a.in, a.Kpad, NP);
+  if (!e) e = encode_state_map(&k.map_acc, a.acc, a.Kpad, NP);
+  if (!e) e = encode_state_map(&k.map_base, a.base, a.Kpad, NP);
+  if (e) return e;
+  tile_stage_kernel<P, NFQ, MAP><<<grid, 4 * kTileElems, Lay::kBytes, st>>>(k, o);
   return cudaGetLastError();
 }
 

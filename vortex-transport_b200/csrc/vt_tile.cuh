@@ -6,10 +6,10 @@
 // stage update Timestepping.cpp:85-306 / :39-82). The state crosses HBM once
 // per stage:
 //
-//   1. load   the tile's state rows arrive in shared memory by TMA bulk copies
-//             (cp.async.bulk, completion on an mbarrier), each run's issued
-//             when that run finished the previous tile's flux phase; the
-//             side-0 neighbours' side nodes,
+//   1. load   the tile's state arrives in shared memory by one 2-D TMA tensor
+//             copy per run (cp.async.bulk.tensor: 2 Np rows x 32 elements,
+//             completion on an mbarrier), issued when that run finished the
+//             previous tile's flux phase; the side-0 neighbours' side nodes,
 //             the neighbour table and the tile's face list were loaded into
 //             registers during the previous tile as well;
 //   2. traces 4 threads per element, one conserved component each, evaluate
@@ -44,11 +44,17 @@
 // tile's volume phase reads. So the two halves of a block run apart from phase
 // 4 of one tile to the end of the next tile's trace phase.
 //
-// Upcoming rows are also prefetched into L2 (cp.async.bulk.prefetch.L2) one
-// tile ahead and the tile's geometry rows into L1, so no phase waits on HBM.
+// The tile's RK operand rows are prefetched into L2 by tensor prefetches (one
+// per run and vector) when the tile starts, and its geometry rows into L1. One
+// tensor instruction per run replaced 2 Np per-row bulk copies and prefetches
+// (4% faster at 768 x 768, p = 3): the TMA unit's instruction issue, not its
+// bandwidth, was what the per-row form paid for.
 // The reference's mass-inverse apply is folded into D and LIFT on the host.
-// Shared-memory rows are padded by one element so that rows that differ by a
-// multiple of 128 bytes do not fall into the same banks.
+// The face and flux buffers' rows are padded by one element so that rows that
+// differ by a multiple of 128 bytes do not fall into the same banks (the face
+// phase reads several rows and columns per warp instruction); the state tile
+// is dense per run, as the tensor copies write it (each warp instruction reads
+// 32 consecutive elements of one row).
 //
 // Every wait on the mbarrier is bounded; a wait that gives up sets bit 1 of
 // err[3], and the block stops taking tiles. StageArgs::wait_tries and
@@ -70,7 +76,7 @@ struct TileLayout {
   static constexpr int ES = E + 1;  // padded row length (elements)
   static constexpr int kFBDoubles = (3 * 4 * NFQ > NP * 8 ? 3 * 4 * NFQ : NP * 8) * ES;
   // byte offsets into dynamic shared memory, each 16-byte aligned
-  static constexpr int kS = 0;                                   // double2 [2NP][ES]
+  static constexpr int kS = 0;  // double2 [2NP][ES]; the stage kernel's tensor copies use it as [2][2NP][32]
   static constexpr int kH = align16(kS + 2 * NP * ES * 16);      // double2 [2NE][ES]
   static constexpr int kFB = align16(kH + 2 * NE * ES * 16);     // double [3][4][NFQ][ES] | [NP][8][ES]
   static constexpr int kTM = align16(kFB + kFBDoubles * 8);      // double [3][NFQ][NE]
@@ -150,6 +156,38 @@ __device__ __forceinline__ void issue_run_copies(const double2* src, long long K
     for (int r = lane; r < 2 * NP; r += 32) bulk_g2s(S + r * ES + which * kTileRun, src + r * Kpad + start, bytes, bar);
 }
 
+
+// Shared-memory index of (row, element column) of the state tile: each run's
+// tensor box lands dense, [2 Np rows][32 elements] per run.
+template <int NP>
+__device__ __forceinline__ int sidx(int row, int el) {
+  return ((el >> 5) * 2 * NP + row) * kTileRun + (el & (kTileRun - 1));
+}
+
+__device__ __forceinline__ void tensor_g2s(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_addr(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tensor_prefetch_l2(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
+               ::"l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y) : "memory");
+}
+
+// Lane 0 of warp `which` announces the run's box and issues its one tensor copy.
+template <int NP>
+__device__ __forceinline__ void issue_run_tensor_copy(const CUtensorMap* map, const int4 run, int which,
+                                                      double2* S, unsigned long long* bar, int lane, int test_flags) {
+  if (test_flags & kTestNoCopies) return;  // test hook: nothing arrives, every wait gives up
+  if (lane != 0) return;
+  const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+  fence_proxy_async_smem();
+  mbar_arrive_expect_tx(bar, len > 0 ? 2u * NP * kTileRun * 16u : 0u);
+  if (len > 0) tensor_g2s(S + which * 2 * NP * kTileRun, map, 2 * start, 0, bar);
+}
+
 // Barrier of the four warps that hold one run's elements (warps of equal parity).
 __device__ __forceinline__ void run_sync(int t) {
   if ((t >> 5) & 1) asm volatile("bar.sync 2, 128;" ::: "memory");
@@ -179,7 +217,7 @@ __device__ __forceinline__ void pair_traces(const StageOps<P, NFQ>& ops, const d
   constexpr int q0 = HALF * QH, q1 = (HALF + 1) * QH < NFQ ? (HALF + 1) * QH : NFQ;
   double2 u[NP];
 #pragma unroll
-  for (int i = 0; i < NP; ++i) u[i] = S[(2 * i + h) * ES + el];
+  for (int i = 0; i < NP; ++i) u[i] = S[sidx<NP>(2 * i + h, el)];
 #pragma unroll
   for (int s = 0; s < 3; ++s)
 #pragma unroll
@@ -292,7 +330,7 @@ __device__ __forceinline__ void pair_update(const StageArgs& a, int e, int h, do
 template <int P, int NFQ, int MAP>
 // Three 256-thread blocks per SM (<= 80 registers per thread) keep 24 warps
 // resident alongside 3 x ~75 KB of shared memory.
-__global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const StageArgs a,
+__global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __grid_constant__ StageArgs a,
                                                                         const StageOps<P, NFQ> ops) {
   using L = TileLayout<P, NFQ>;
   constexpr int E = L::E;
@@ -301,7 +339,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
   constexpr int ES = L::ES;
   constexpr int T = 4 * E;
   constexpr bool PAIR = MAP == kMapPair;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   double2* S = reinterpret_cast<double2*>(smem + L::kS);
   double2* H = reinterpret_cast<double2*>(smem + L::kH);
   double* FB = reinterpret_cast<double*>(smem + L::kFB);
@@ -350,7 +388,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       hreg[k] = (valid && r < 2 * NE) ? __ldg(a.in + r * KP + my_nb.x) : make_double2(1.0, 0.0);
     }
   }
-  if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, run, t >> 5, S, bar, lane, a.test_flags);
+  if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, run, t >> 5, S, bar, lane, a.test_flags);
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
@@ -360,16 +398,12 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
     // geometry rows into L1. The next tile's state is not prefetched: its bulk
     // copies, issued in phase 5, read it from HBM themselves (prefetching it
     // as well was 1.6% slower) -------------------------------------------------
-    if (t >= 64 && t < 64 + 8 * NP) {
-      const int l = t - 64, which = l & 1, r = l >> 1;
+    if (t >= 64 && t < 68) {
+      const int which = t & 1, vec = (t - 64) >> 1;  // vec 0: acc, 1: base
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
       if (len > 0) {
-        const unsigned bytes = static_cast<unsigned>(len) * 16u;
-        if (r < 2 * NP) {
-          if (a.stage >= 1 && a.stage <= 3) prefetch_l2(a.acc + r * KP + start, bytes);
-        } else if (a.stage == 1 || a.stage == 2) {
-          prefetch_l2(a.base + (r - 2 * NP) * KP + start, bytes);
-        }
+        if (vec == 0 && a.stage >= 1 && a.stage <= 3) tensor_prefetch_l2(&a.map_acc, 2 * start, 0);
+        if (vec == 1 && (a.stage == 1 || a.stage == 2)) tensor_prefetch_l2(&a.map_base, 2 * start, 0);
       }
     } else if (t >= 64 + 8 * NP && t < 64 + 8 * NP + 56) {
       // this tile's 7 geometry rows into L1 (4 lines per 32-element run)
@@ -415,7 +449,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       const double* Sd = reinterpret_cast<const double*>(S);
       double u[NP];
 #pragma unroll
-      for (int i = 0; i < NP; ++i) u[i] = Sd[((2 * i + (cc >> 1)) * ES + el) * 2 + (cc & 1)];
+      for (int i = 0; i < NP; ++i) u[i] = Sd[sidx<NP>(2 * i + (cc >> 1), el) * 2 + (cc & 1)];
 #pragma unroll
       for (int s = 0; s < 3; ++s)
 #pragma unroll
@@ -551,7 +585,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
       const double2 j0 = __ldg(a.geo + 0 * KP + eg);
       const double2 j1 = __ldg(a.geo + 1 * KP + eg);
       for (int j = grp; j < NP; j += 4) {
-        const double2 s0 = S[(2 * j) * ES + el], s1 = S[(2 * j + 1) * ES + el];
+        const double2 s0 = S[sidx<NP>(2 * j, el)], s1 = S[sidx<NP>(2 * j + 1, el)];
         const double sv[4] = {s0.x, s0.y, s1.x, s1.y};
         double gxi[4], geta[4];
         contravariant_flux(sv, j0.x, j0.y, j1.x, j1.y, gxi, geta);
@@ -573,7 +607,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const Sta
 
     // this run's columns of the state tile are free: start its next copies and neighbour rows
     if (has_next) {
-      if (t < 64) issue_run_copies<NP, ES>(a.in, a.Kpad, next_run, t >> 5, S, bar, lane, a.test_flags);
+      if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, next_run, t >> 5, S, bar, lane, a.test_flags);
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       const bool nvalid = pos < (second ? next_run.w : next_run.y);
