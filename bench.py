@@ -58,8 +58,9 @@ def load_peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per stage launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "stage_kernel_p3_traffic.txt")
+    """DRAM bytes per stage launch at 768x768 from the committed full-size ncu capture
+    (profiles/tile_stage_kernel_p3_768x768_traffic.txt), if present."""
+    path = os.path.join(ROOT, "profiles", "tile_stage_kernel_p3_768x768_traffic.txt")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch_full_size:"):
