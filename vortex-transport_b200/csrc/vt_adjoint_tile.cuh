@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
   constexpr int NE = B::NE;
   constexpr int ES = B::ES;
   constexpr int T = 4 * E;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   double2* S = reinterpret_cast<double2*>(smem + B::kS);
   double2* H = reinterpret_cast<double2*>(smem + B::kH);
   double* FB = reinterpret_cast<double*>(smem + B::kFB);

@@ -10,8 +10,10 @@
 //             copy per run (cp.async.bulk.tensor: 2 Np rows x 32 elements,
 //             completion on an mbarrier), issued when that run finished the
 //             previous tile's flux phase; the side-0 neighbours' side nodes,
-//             the neighbour table and the tile's face list were loaded into
-//             registers during the previous tile as well;
+//             the neighbour table and the tile's face list were copied into
+//             shared memory during the previous tile as well, by cp.async
+//             (global to shared without registers), once the previous tile's
+//             faces no longer needed those buffers;
 //   2. traces 4 threads per element, one conserved component each, evaluate
 //             the element's own trace at every face point from the p+1 side
 //             nodes (coefficients are immediates);
@@ -43,6 +45,16 @@
 // same elements, and the next tile's traces reuse rows of the buffer that this
 // tile's volume phase reads. So the two halves of a block run apart from phase
 // 4 of one tile to the end of the next tile's trace phase.
+//
+// Registers are the kernel's scarcest resource (80 per thread for three blocks
+// per SM), so nothing about the next tile is held in registers across a tile:
+// its neighbour rows, neighbour table and face list go straight to shared
+// memory by cp.async, and the tile descriptor (the two runs) is kept in shared
+// memory, one copy per run, written after the face phase by the run's first
+// warp and read behind the run's own barriers. Holding them in registers cost
+// 176 bytes of spill stores per thread, whose reloads missed the small L1 that
+// three 73 KB blocks leave; staged this way 16 bytes remain and a step at
+// 768 x 768, p = 3 is 12% faster, with bit-identical results.
 //
 // The tile's RK operand rows are prefetched into L2 by tensor prefetches (one
 // per run and vector) when the tile starts, and its geometry rows into L1. One
@@ -84,7 +96,8 @@ struct TileLayout {
   static constexpr int kEL = align16(kNB + E * 16);              // int [E] global element index
   static constexpr int kItems = align16(kEL + E * 4);            // int [kMaxItems]
   static constexpr int kBar = align16(kItems + kMaxItems * 4);   // mbarrier (8 B) + abort flag
-  static constexpr int kBytes = align16(kBar + 16);
+  static constexpr int kRuns = kBar + 16;                        // int4 [2] tile descriptor, one copy per run
+  static constexpr int kBytes = align16(kRuns + 32);
 };
 
 // ---- TMA unit ------------------------------------------------------------------
@@ -131,6 +144,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
+
+// Global-to-shared copies that bypass the registers (cp.async, completed per
+// thread by cp.async.wait_all): 16 bytes (both addresses 16-byte aligned,
+// cached in L2 only) or 4 bytes.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(__cvta_generic_to_global(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(__cvta_generic_to_global(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -350,6 +377,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
   int* items = reinterpret_cast<int*>(smem + L::kItems);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + L::kBar);
   int* abort_flag = reinterpret_cast<int*>(smem + L::kBar + 8);
+  int4* RUNS = reinterpret_cast<int4*>(smem + L::kRuns);
 
   const int t = threadIdx.x;
   const int col = t % E, grp = t / E;  // load mapping; also (element, group) later
@@ -368,31 +396,42 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
   }
   __syncthreads();
 
-  // tile metadata of the tile in hand: run, face count, this thread's face
-  // item, this column's neighbours and side-0 neighbour rows
+  // the first tile: its descriptor (one copy per run), face count, and by
+  // cp.async its face list, neighbour table and side-0 neighbour rows; then
+  // its state copies
   int tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  int4 run = __ldg(a.tiles + tile);
   int nitems = __ldg(a.tile_count + tile);
-  int my_item = t < kMaxItems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
-  int4 my_nb = make_int4(0, 0, 0, 0);
-  double2 hreg[2];
   {
+    const int4 run = __ldg(a.tiles + tile);
+    if (lane == 0 && t < 64) RUNS[t >> 5] = run;
     const int pos = col % kTileRun;
     const bool second = col >= kTileRun;
     const bool valid = pos < (second ? run.w : run.y);
-    if (valid) my_nb = __ldg(a.nbr + (second ? run.z : run.x) + pos);
+    const int4* nsrc = a.nbr + (second ? run.z : run.x) + pos;
+    const int nbx = valid ? __ldg(&nsrc->x) : 0;
+    if (grp == 0) {
+      if (valid) cp_async16(NB + col, nsrc);
+      else NB[col] = make_int4(0, 0, 0, 0);
+    }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int r = grp + 4 * k;
-      hreg[k] = (valid && r < 2 * NE) ? __ldg(a.in + r * KP + my_nb.x) : make_double2(1.0, 0.0);
+      if (r < 2 * NE) {
+        if (valid) cp_async16(H + r * ES + col, a.in + r * KP + nbx);
+        else H[r * ES + col] = make_double2(1.0, 0.0);
+      }
     }
+    if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile) * kMaxItems + t);
+    cp_async_commit();
+    if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, run, t >> 5, S, bar, lane, a.test_flags);
   }
-  if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, run, t >> 5, S, bar, lane, a.test_flags);
+  __syncthreads();
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
     const bool has_next = tile + G < a.ntiles;
+    const int4 run = RUNS[(t >> 5) & 1];
 
     // ---- prefetch: this tile's RK operand rows into L2 (read in phase 6) and its
     // geometry rows into L1. The next tile's state is not prefetched: its bulk
@@ -419,16 +458,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
       const bool valid = pos < (second ? run.w : run.y);
-      if (grp == 0) {
-        NB[col] = my_nb;
-        EL[col] = valid ? (second ? run.z : run.x) + pos : -1;
-      }
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int r = grp + 4 * k;
-        if (r < 2 * NE) H[r * ES + col] = hreg[k];
-      }
-      if (t < nitems) items[t] = my_item;
+      if (grp == 0) EL[col] = valid ? (second ? run.z : run.x) + pos : -1;
     }
     {
       bool ok = false;
@@ -460,6 +490,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
           FB[((s * 4 + cc) * NFQ + q) * ES + el] = v;
         }
     }
+    cp_async_wait_all();  // this thread's cp.async copies of the tile's face list and neighbour rows
     __syncthreads();
     if (*abort_flag) break;
 
@@ -533,22 +564,34 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     }
     __syncthreads();
 
-    // next tile's metadata (next_run has arrived by now); the item rows are
-    // kMaxItems wide, so the load need not wait for the item count
+    // next tile's metadata (next_run has arrived by now). The face list,
+    // neighbour table and element indices of this tile are no longer read, so
+    // the next tile's go to shared memory now; the item rows are kMaxItems
+    // wide, so the copy need not wait for the item count. The descriptor
+    // copies are read again after this run's next barrier (by the copy issue
+    // below and at the next tile's start).
+    int nbx = 0;
+    bool nvalid = false;
+    if (lane == 0 && t < 64) RUNS[t >> 5] = next_run;
     if (has_next) {
       nitems = __ldg(a.tile_count + tile + G);
-      my_item = t < kMaxItems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
+      if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t);
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
-      my_nb = pos < (second ? next_run.w : next_run.y) ? __ldg(a.nbr + (second ? next_run.z : next_run.x) + pos)
-                                                       : make_int4(0, 0, 0, 0);
+      nvalid = pos < (second ? next_run.w : next_run.y);
+      const int4* nsrc = a.nbr + (second ? next_run.z : next_run.x) + pos;
+      nbx = nvalid ? __ldg(&nsrc->x) : 0;
+      if (grp == 0) {
+        if (nvalid) cp_async16(NB + col, nsrc);
+        else NB[col] = make_int4(0, 0, 0, 0);
+      }
     }
 
     // ---- 4. lift ---------------------------------------------------------------------------
     const int el = col;
     const int e = EL[el];
     const bool valid = e >= 0;
-    const int eg = valid ? e : run.x;
+    const int eg = valid ? e : 0;
     constexpr int NH = (NP + 1) / 2;
     constexpr int NR = PAIR ? NH : NP;  // accumulators: double2 per node pair, or one double per node
     double2 r2[PAIR ? NH : 1];
@@ -607,16 +650,17 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
 
     // this run's columns of the state tile are free: start its next copies and neighbour rows
     if (has_next) {
-      if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, next_run, t >> 5, S, bar, lane, a.test_flags);
-      const int pos = col % kTileRun;
-      const bool second = col >= kTileRun;
-      const bool nvalid = pos < (second ? next_run.w : next_run.y);
+      if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, RUNS[t >> 5], t >> 5, S, bar, lane, a.test_flags);
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const int rr = grp + 4 * k;
-        hreg[k] = (nvalid && rr < 2 * NE) ? __ldg(a.in + rr * KP + my_nb.x) : make_double2(1.0, 0.0);
+        if (rr < 2 * NE) {
+          if (nvalid) cp_async16(H + rr * ES + col, a.in + rr * KP + nbx);
+          else H[rr * ES + col] = make_double2(1.0, 0.0);
+        }
       }
     }
+    cp_async_commit();
 
     // the stage update's first operand, requested now so that it is in flight
     // during the volume phase
@@ -695,13 +739,13 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
         }
       }
     }
-    run = next_run;
     // the four warps of a run work on the same elements: none may start the
     // next tile's traces (which reuse rows of the face / flux buffer) before
     // the others are done with this tile's volume phase
     run_sync(t);
   }
 
+  cp_async_wait_all();  // none may land after the block has left
   if (*abort_flag) {
     // the bulk copies of a tile whose wait gave up may still land: wait for
     // them once more, with the same bound, before the block leaves
