@@ -145,10 +145,16 @@ struct AdjointState {
   AdjKernels k;
   SweepGraph fwd_graph, bwd_graph;
   size_t state_elems = 0;  // double2 entries of one state vector
-  // work, stage states, adjoint, accumulator, two stage adjoints (contiguous)
+  // work, stage states, adjoint, accumulator, two stage adjoints, second set
+  // of stage states (contiguous)
   double2* bufs = nullptr;
   double2 *work = nullptr, *s1 = nullptr, *s2 = nullptr, *s3 = nullptr;
   double2 *lam = nullptr, *acc = nullptr, *a0 = nullptr, *a1 = nullptr;
+  double2 *t1 = nullptr, *t2 = nullptr, *t3 = nullptr;
+  // the reverse sweep's recomputation runs on `side`, ahead of the reverse
+  // steps on the context's stream (run_plan_overlapped)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ready[2] = {nullptr, nullptr}, ev_freed[2] = {nullptr, nullptr};
   double2 *bp = nullptr, *bm = nullptr;  // face adjoints of the two-launch form (else null)
   // fused reverse stage (adjoint_tile_kernel): persistent grid size, 0 when
   // the edge-once form does not apply (the element adjacency does not
@@ -168,6 +174,14 @@ struct AdjointState {
 };
 
 namespace {
+
+void release_streams(AdjointState* s) {
+  cudaEvent_t evs[6] = {s->ev_fork, s->ev_join, s->ev_ready[0], s->ev_ready[1], s->ev_freed[0], s->ev_freed[1]};
+  for (cudaEvent_t ev : evs)
+    if (ev) cudaEventDestroy(ev);
+  if (s->side) cudaStreamDestroy(s->side);
+  s->side = nullptr;
+}
 
 int setup(vt_ctx* c) {
   if (c->adj) return VT_OK;
@@ -211,11 +225,12 @@ int setup(vt_ctx* c) {
       tile_blocks = sms * per_sm;
     cudaGetLastError();
   }
-  // eight state vectors, plus the face adjoints of the two-launch form when
+  // eleven state vectors, plus the face adjoints of the two-launch form when
   // that form is the one used
+  constexpr int kVectors = 11;
   const size_t state_elems = static_cast<size_t>(2 * c->Np) * static_cast<size_t>(c->Kpad);
   const size_t face_elems = tile_blocks > 0 ? 0 : static_cast<size_t>(6 * c->nfq) * static_cast<size_t>(c->Kpad);
-  const size_t total = 8 * state_elems + 2 * face_elems;
+  const size_t total = kVectors * state_elems + 2 * face_elems;
   double2* bufs = nullptr;
   e = cudaMalloc(reinterpret_cast<void**>(&bufs), sizeof(double2) * total);
   if (!e) e = cudaMemsetAsync(bufs, 0, sizeof(double2) * total, c->stream);
@@ -225,14 +240,25 @@ int setup(vt_ctx* c) {
     return fail(e == cudaErrorMemoryAllocation ? VT_ERR_NO_MEMORY : VT_ERR_CUDA, cuda_msg("adjoint buffers", e));
   }
   auto* s = new AdjointState();
+  e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+  cudaEvent_t* evs[6] = {&s->ev_fork, &s->ev_join, &s->ev_ready[0], &s->ev_ready[1], &s->ev_freed[0], &s->ev_freed[1]};
+  for (int i = 0; i < 6 && !e; ++i) e = cudaEventCreateWithFlags(evs[i], cudaEventDisableTiming);
+  if (e) {
+    cudaGetLastError();
+    release_streams(s);
+    delete s;
+    cudaFree(bufs);
+    return fail(VT_ERR_CUDA, cuda_msg("adjoint streams", e));
+  }
   s->k = k;
   s->tile_blocks = tile_blocks;
   s->state_elems = state_elems;
   s->bufs = bufs;
-  double2** named[8] = {&s->work, &s->s1, &s->s2, &s->s3, &s->lam, &s->acc, &s->a0, &s->a1};
-  for (int i = 0; i < 8; ++i) *named[i] = s->bufs + i * s->state_elems;
+  double2** named[kVectors] = {&s->work, &s->s1, &s->s2, &s->s3, &s->lam, &s->acc,
+                                &s->a0,   &s->a1, &s->t1, &s->t2, &s->t3};
+  for (int i = 0; i < kVectors; ++i) *named[i] = s->bufs + i * s->state_elems;
   if (face_elems) {
-    s->bp = s->bufs + 8 * s->state_elems;
+    s->bp = s->bufs + kVectors * s->state_elems;
     s->bm = s->bp + face_elems;
   }
   c->adj = s;
@@ -259,8 +285,9 @@ double2* slot(vt_ctx* c, long long i) {
   return i == kWorkSlot ? c->adj->work : c->adj->slots + static_cast<size_t>(i) * c->adj->state_elems;
 }
 
-cudaError_t stage(vt_ctx* c, const double2* in, const double2* base, double2* out, int st, double ca, double co) {
-  return c->launch(stage_args(c, in, base, c->A, out, st, ca, co), c->ops.data(), c->max_blocks, c->stream);
+cudaError_t stage(vt_ctx* c, const double2* in, const double2* base, double2* out, int st, double ca, double co,
+                  cudaStream_t stream) {
+  return c->launch(stage_args(c, in, base, c->A, out, st, ca, co), c->ops.data(), c->max_blocks, stream);
 }
 
 // The step size the coefficients carry: dt, or 1 when the device scales them
@@ -268,35 +295,35 @@ cudaError_t stage(vt_ctx* c, const double2* in, const double2* base, double2* ou
 double dt_scale(const vt_ctx* c, double dt) { return c->tile_dt ? 1.0 : dt; }
 
 // One plain RK4 step from X into Y (Y may be X), stages through Sa, Sb.
-cudaError_t plain_step(vt_ctx* c, const double2* X, double2* Y, double dt0) {
+cudaError_t plain_step(vt_ctx* c, const double2* X, double2* Y, double dt0, cudaStream_t st) {
   const double dt = dt_scale(c, dt0);
   cudaError_t e;
-  if ((e = stage(c, X, X, c->Sa, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
-  if ((e = stage(c, c->Sa, X, c->Sb, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
-  if ((e = stage(c, c->Sb, X, c->Sa, 2, (1.0 / 3) * dt, dt))) return e;
-  return stage(c, c->Sa, X, Y, 3, 0.0, (1.0 / 6) * dt);
+  if ((e = stage(c, X, X, c->Sa, 0, (1.0 / 6) * dt, 0.5 * dt, st))) return e;
+  if ((e = stage(c, c->Sa, X, c->Sb, 1, (1.0 / 3) * dt, 0.5 * dt, st))) return e;
+  if ((e = stage(c, c->Sb, X, c->Sa, 2, (1.0 / 3) * dt, dt, st))) return e;
+  return stage(c, c->Sa, X, Y, 3, 0.0, (1.0 / 6) * dt, st);
 }
 
-cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt) {
-  cudaError_t e = plain_step(c, X, Y, dt);
-  for (int i = 1; i < k && !e; ++i) e = plain_step(c, Y, Y, dt);
+cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt, cudaStream_t st) {
+  cudaError_t e = plain_step(c, X, Y, dt, st);
+  for (int i = 1; i < k && !e; ++i) e = plain_step(c, Y, Y, dt, st);
   return e;
 }
 
 // Step from X keeping the stage states in S1, S2, S3; the new state goes to
 // `out` when given (else the last stage is not run).
 cudaError_t stage_step(vt_ctx* c, const double2* X, double2* S1, double2* S2, double2* S3, double dt0,
-                       double2* out) {
+                       double2* out, cudaStream_t st) {
   const double dt = dt_scale(c, dt0);
   cudaError_t e;
-  if ((e = stage(c, X, X, S1, 0, (1.0 / 6) * dt, 0.5 * dt))) return e;
-  if ((e = stage(c, S1, X, S2, 1, (1.0 / 3) * dt, 0.5 * dt))) return e;
-  if ((e = stage(c, S2, X, S3, 2, (1.0 / 3) * dt, dt))) return e;
-  return out ? stage(c, S3, X, out, 3, 0.0, (1.0 / 6) * dt) : cudaSuccess;
+  if ((e = stage(c, X, X, S1, 0, (1.0 / 6) * dt, 0.5 * dt, st))) return e;
+  if ((e = stage(c, S1, X, S2, 1, (1.0 / 3) * dt, 0.5 * dt, st))) return e;
+  if ((e = stage(c, S2, X, S3, 2, (1.0 / 3) * dt, dt, st))) return e;
+  return out ? stage(c, S3, X, out, 3, 0.0, (1.0 / 6) * dt, st) : cudaSuccess;
 }
 
 cudaError_t stage_step(vt_ctx* c, const double2* X, double dt, double2* out) {
-  return stage_step(c, X, c->adj->s1, c->adj->s2, c->adj->s3, dt, out);
+  return stage_step(c, X, c->adj->s1, c->adj->s2, c->adj->s3, dt, out, c->stream);
 }
 
 AdjArgs adj_args(vt_ctx* c) {
@@ -354,7 +381,7 @@ cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
   for (size_t i = begin; i < end && !e; ++i) {
     const CkptAction& a = s->plan[i];
     switch (a.op) {
-      case CkptOp::kAdvance: e = advance(c, slot(c, a.src), a.steps, slot(c, a.dst), s->dt); break;
+      case CkptOp::kAdvance: e = advance(c, slot(c, a.src), a.steps, slot(c, a.dst), s->dt, c->stream); break;
       case CkptOp::kStageStep:
         e = stage_step(c, slot(c, a.src), s->dt, a.step == s->nsteps - 1 ? out_last : nullptr);
         break;
@@ -362,6 +389,65 @@ cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
     }
   }
   return e;
+}
+
+// Runs plan[begin, end) of a reverse sweep with the recomputation one step
+// ahead: advances and stage steps go to the side stream, reverse steps stay on
+// the context's stream, and the stage states alternate between two sets, so
+// that the recomputation of step i-1 overlaps the reverse of step i (at small
+// sizes neither kernel fills the GPU; a tile kernel's last round of tiles
+// leaves most SMs idle). The order the single-stream plan implies is kept by
+// events: a reverse step waits for the stage step that wrote its set; a stage
+// step waits until the reverse step that read the set it overwrites is done;
+// an advance that overwrites a slot a reverse step issued before still reads
+// waits for the reverse steps issued so far. Both streams run the same
+// launches as run_plan, so the results are identical. Must be called inside a
+// stream capture of the context's stream; set 0 (s1..s3) holds the stage
+// states of the plan's first reverse step on entry.
+cudaError_t run_plan_overlapped(vt_ctx* c, size_t begin, size_t end) {
+  AdjointState* s = c->adj;
+  cudaStream_t M = c->stream, R = s->side;
+  double2* const sets[2][3] = {{s->s1, s->s2, s->s3}, {s->t1, s->t2, s->t3}};
+  bool ready_rec[2] = {false, false};  // ev_ready[k] recorded in this capture
+  bool freed_rec[2] = {false, false};  // ev_freed[k] recorded (a reverse step read set k)
+  int cur = 0;                         // the set the last stage step wrote
+  int last_read = -1;                  // the set of the last reverse step issued, or -1
+  std::vector<long long> pending;      // slots read by reverse steps since R last waited for M
+  cudaError_t e = cudaEventRecord(s->ev_fork, M);
+  if (!e) e = cudaStreamWaitEvent(R, s->ev_fork, 0);
+  for (size_t i = begin; i < end && !e; ++i) {
+    const CkptAction& a = s->plan[i];
+    switch (a.op) {
+      case CkptOp::kAdvance:
+        if (last_read >= 0 && std::find(pending.begin(), pending.end(), static_cast<long long>(a.dst)) != pending.end()) {
+          e = cudaStreamWaitEvent(R, s->ev_freed[last_read], 0);
+          pending.clear();
+        }
+        if (!e) e = advance(c, slot(c, a.src), a.steps, slot(c, a.dst), s->dt, R);
+        break;
+      case CkptOp::kStageStep: {
+        const int w = cur ^ 1;
+        if (freed_rec[w]) e = cudaStreamWaitEvent(R, s->ev_freed[w], 0);
+        if (!e) e = stage_step(c, slot(c, a.src), sets[w][0], sets[w][1], sets[w][2], s->dt, nullptr, R);
+        if (!e) e = cudaEventRecord(s->ev_ready[w], R);
+        ready_rec[w] = true;
+        cur = w;
+        break;
+      }
+      case CkptOp::kAdjoint:
+        if (ready_rec[cur]) e = cudaStreamWaitEvent(M, s->ev_ready[cur], 0);
+        if (!e) e = adjoint_step(c, slot(c, a.src), sets[cur][0], sets[cur][1], sets[cur][2], s->dt);
+        if (!e) e = cudaEventRecord(s->ev_freed[cur], M);
+        freed_rec[cur] = true;
+        last_read = cur;
+        pending.push_back(a.src);
+        break;
+    }
+  }
+  // the side stream rejoins the capture's origin stream
+  const cudaError_t j = cudaEventRecord(s->ev_join, R);
+  const cudaError_t k = j ? j : cudaStreamWaitEvent(M, s->ev_join, 0);
+  return e ? e : k;
 }
 
 // Host or device AoS array -> SoA buffer on the context's stream.
@@ -438,6 +524,7 @@ void adjoint_release(vt_ctx* c) {
   c->adj->bwd_graph.reset();
   if (c->adj->slots) cudaFree(c->adj->slots);
   if (c->adj->bufs) cudaFree(c->adj->bufs);
+  release_streams(c->adj);
   delete c->adj;
   c->adj = nullptr;
 }
@@ -475,7 +562,8 @@ int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
                                         cudaMemcpyDeviceToDevice, c->stream);
         for (int i = 0; i < nsteps && !x; ++i)
           x = vt::stage_step(c, vt::slot(c, 4ll * i), vt::slot(c, 4ll * i + 1), vt::slot(c, 4ll * i + 2),
-                             vt::slot(c, 4ll * i + 3), dt, i + 1 < nsteps ? vt::slot(c, 4ll * i + 4) : c->U);
+                             vt::slot(c, 4ll * i + 3), dt, i + 1 < nsteps ? vt::slot(c, 4ll * i + 4) : c->U,
+                             c->stream);
         return x;
       });
     if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint forward", e));
@@ -536,7 +624,7 @@ int vt_adjoint_backward(vt_ctx* c, const double* dJdU_T, double* dJdU_0, int dev
   if (!e) e = vt::load_aos(c, dJdU_T, device_pointers, s->lam);
   if (!e)
     e = vt::run_captured(c, s->bwd_graph, vt::sweep_key(c, 3),
-                         [&]() { return vt::run_plan(c, s->first_adjoint, s->plan.size(), nullptr); });
+                         [&]() { return vt::run_plan_overlapped(c, s->first_adjoint, s->plan.size()); });
   if (!e) e = vt::store_aos(c, s->lam, dJdU_0, device_pointers);
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("adjoint backward", e));
   return vt::finish(c, 0, 0.0);
@@ -626,7 +714,7 @@ int vt_tangent_rk4(vt_ctx* c, double dt, int nsteps, const double* dU_0, double*
         (e = vt::lincomb(c, dS, dX, 1.0, dk, dt)))
       break;
     if ((e = jvp(s->s3, dS)) || (e = vt::lincomb(c, dX, dacc, 1.0, dk, (1.0 / 6) * dt))) break;
-    e = vt::stage(c, s->s3, X, c->U, 3, 0.0, (1.0 / 6) * dt);
+    e = vt::stage(c, s->s3, X, c->U, 3, 0.0, (1.0 / 6) * dt, c->stream);
   }
   if (!e) e = vt::store_aos(c, dX, dU_T, device_pointers);
   if (e) return fail(VT_ERR_CUDA, vt::cuda_msg("tangent", e));
