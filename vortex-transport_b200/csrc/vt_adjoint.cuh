@@ -317,7 +317,7 @@ __host__ __device__ inline void roe_flux_vjp(const double* uL, const double* uR,
   const double b_HR = b_Hi * di * d1, b_HL = b_Hi * d1;
   // d1 = 1 / (1 + di); di = sqrt(rR irL)
   b_di -= b_d1 * d1 * d1;
-  const double b_q = b_di * 0.5 / di;
+  const double b_q = b_di * 0.5 * rcp(di);
   double b_rR = b_q * irL;
   double b_irL = b_q * rR;
   // du = uR - uL

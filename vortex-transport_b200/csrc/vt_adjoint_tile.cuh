@@ -137,35 +137,6 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
   for (; tile < a.ntiles; tile += G) {
     const bool has_next = tile + G < a.ntiles;
 
-    // ---- prefetch into L2: the next tile's state, geometry, neighbour and
-    // adjoint rows; this tile's lam / acc_in rows (read in phase 6) -------------
-    if (t < 64) {
-      if (has_next) {
-        const int4 rr = __ldg(a.tiles + tile + G);
-        const int which = t & 1, r = t >> 1;
-        const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
-        if (len > 0) {
-          const unsigned bytes = static_cast<unsigned>(len) * 16u;
-          if (r < 2 * NP) prefetch_l2(a.U + r * KP + start, bytes);
-          else if (r < 2 * NP + 7) prefetch_l2(a.geo + (r - 2 * NP) * KP + start, bytes);
-          else if (r == 2 * NP + 7) prefetch_l2(a.nbr + start, bytes);
-        }
-      }
-    } else if (t < 64 + 8 * NP) {
-      const int l = t - 64, which = l & 1, r = l >> 1;
-      if (r < 2 * NP) {
-        if (has_next) {
-          const int4 rr = __ldg(a.tiles + tile + G);
-          const int start = which ? rr.z : rr.x, len = which ? rr.w : rr.y;
-          if (len > 0) prefetch_l2(a.a + r * KP + start, static_cast<unsigned>(len) * 16u);
-        }
-      } else {
-        const int start = which ? run.z : run.x, len = which ? run.w : run.y;
-        const double2* src = a.lam ? a.lam : a.acc_in;
-        if (len > 0 && src) prefetch_l2(src + (r - 2 * NP) * KP + start, static_cast<unsigned>(len) * 16u);
-      }
-    }
-
     // ---- 1. load ------------------------------------------------------------------
     int4 next_run = make_int4(0, 0, 0, 0);
     if (has_next) next_run = __ldg(a.tiles + tile + G);
