@@ -367,14 +367,23 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       const double* accp = reinterpret_cast<const double*>(a.acc_in);
       double* acco = reinterpret_cast<double*>(a.acc_out);
       double* aout = reinterpret_cast<double*>(a.a_out);
+      // every load before the first store: acc_in and acc_out are the same
+      // array in three of the four reverse stages, so loads that follow a
+      // store could not be moved above it and each would wait on its own
+      // round trip to L2 (this phase took a quarter of the kernel's time)
+      double lv[NP], av[NP];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const long long x = comp_index(KP, i, c, e);
+        lv[i] = need_lam ? lamp[x] : 0.0;
+        av[i] = accp ? accp[x] : 0.0;
+      }
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
         const long long x = comp_index(KP, i, c, e);
         const double gi = P > 0 ? g[i] + Gs[(i * 8 + c) * ES + el] : g[i];
-        const double l = need_lam ? lamp[x] : 0.0;
-        const double ai = accp ? accp[x] : 0.0;
-        acco[x] = fma(a.lam_coef, l, ai) + gi;
-        if (aout) aout[x] = fma(cl, l, cg * gi);
+        acco[x] = fma(a.lam_coef, lv[i], av[i]) + gi;
+        if (aout) aout[x] = fma(cl, lv[i], cg * gi);
       }
     }
     run = next_run;

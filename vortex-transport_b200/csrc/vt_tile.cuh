@@ -329,28 +329,39 @@ __device__ __forceinline__ void pair_update(const StageArgs& a, int e, int h, do
   constexpr int NP = np_of_p(P), NH = (NP + 1) / 2;
   const long long KP = a.Kpad;
   const long long o = (2 * HALF * NH + h) * KP + e;  // row 2 * node + h of this half's first node
+  constexpr int N = NP - HALF * NH < NH ? NP - HALF * NH : NH;  // nodes of this half
+  switch (a.stage) {
+    case 0:
 #pragma unroll
-  for (int i = 0; i < NH; ++i) {
-    if (HALF * NH + i >= NP) break;
-    const long long x = o + i * 2 * KP;
-    switch (a.stage) {
-      case 0:
-        a.acc[x] = fma2(c_acc, r[i], pre[i]);
-        a.out[x] = fma2(c_out, r[i], pre[i]);
-        break;
-      case 1:
-      case 2:
-        a.acc[x] = fma2(c_acc, r[i], a.acc[x]);
-        a.out[x] = fma2(c_out, r[i], pre[i]);
-        break;
-      case 3:
-      case kStageEuler:
-        a.out[x] = fma2(c_out, r[i], pre[i]);
-        break;
-      default:
-        a.out[x] = r[i];
-        break;
+      for (int i = 0; i < N; ++i) {
+        a.acc[o + i * 2 * KP] = fma2(c_acc, r[i], pre[i]);
+        a.out[o + i * 2 * KP] = fma2(c_out, r[i], pre[i]);
+      }
+      break;
+    case 1:
+    case 2: {
+      // every accumulator row is read before the first store: a load that
+      // follows a store to another array cannot be moved above it, so read
+      // and written in turn each row would wait on its own memory round trip
+      double2 av[NH];
+#pragma unroll
+      for (int i = 0; i < N; ++i) av[i] = a.acc[o + i * 2 * KP];
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        a.acc[o + i * 2 * KP] = fma2(c_acc, r[i], av[i]);
+        a.out[o + i * 2 * KP] = fma2(c_out, r[i], pre[i]);
+      }
+      break;
     }
+    case 3:
+    case kStageEuler:
+#pragma unroll
+      for (int i = 0; i < N; ++i) a.out[o + i * 2 * KP] = fma2(c_out, r[i], pre[i]);
+      break;
+    default:
+#pragma unroll
+      for (int i = 0; i < N; ++i) a.out[o + i * 2 * KP] = r[i];
+      break;
   }
 }
 
@@ -720,13 +731,17 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
             }
             break;
           case 1:
-          case 2:
+          case 2: {
+            double av[NP];  // all reads before the first store, as in pair_update
+#pragma unroll
+            for (int i = 0; i < NP; ++i) av[i] = acc[i * step];
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
-              acc[i * step] = fma(c_acc, r[i], acc[i * step]);
+              acc[i * step] = fma(c_acc, r[i], av[i]);
               out[i * step] = fma(c_out, r[i], pre[i]);
             }
             break;
+          }
           case 3:
           case kStageEuler:
 #pragma unroll
