@@ -581,19 +581,14 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     // wide, so the copy need not wait for the item count. The descriptor
     // copies are read again after this run's next barrier (by the copy issue
     // below and at the next tile's start).
-    int nbx = 0;
-    bool nvalid = false;
     if (lane == 0 && t < 64) RUNS[t >> 5] = next_run;
     if (has_next) {
       nitems = __ldg(a.tile_count + tile + G);
       if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t);
-      const int pos = col % kTileRun;
-      const bool second = col >= kTileRun;
-      nvalid = pos < (second ? next_run.w : next_run.y);
-      const int4* nsrc = a.nbr + (second ? next_run.z : next_run.x) + pos;
-      nbx = nvalid ? __ldg(&nsrc->x) : 0;
       if (grp == 0) {
-        if (nvalid) cp_async16(NB + col, nsrc);
+        const int pos = col % kTileRun;
+        const bool second = col >= kTileRun;
+        if (pos < (second ? next_run.w : next_run.y)) cp_async16(NB + col, a.nbr + (second ? next_run.z : next_run.x) + pos);
         else NB[col] = make_int4(0, 0, 0, 0);
       }
     }
@@ -632,6 +627,9 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
       }
     }
     (void)NR;
+    // the next tile's neighbour table has landed (its copies were issued before
+    // the lift); the run's barrier makes it visible to the column's other threads
+    if (grp == 0) cp_async_wait_all();
     run_sync(t);
 
     // ---- 5. nodal flux of every node, once, contracted with the inverse Jacobian --------
@@ -662,6 +660,12 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     // this run's columns of the state tile are free: start its next copies and neighbour rows
     if (has_next) {
       if (t < 64) issue_run_tensor_copy<NP>(&a.map_in, RUNS[t >> 5], t >> 5, S, bar, lane, a.test_flags);
+      // the next tile's side-0 neighbours, from the descriptor and neighbour
+      // table already in shared memory (held in registers across the lift and
+      // the nodal flux they were spilled, and their global load waited on)
+      const int4 nr = RUNS[col >= kTileRun];
+      const bool nvalid = col % kTileRun < (col >= kTileRun ? nr.w : nr.y);
+      const int nbx = NB[col].x;
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const int rr = grp + 4 * k;
