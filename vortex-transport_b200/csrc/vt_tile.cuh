@@ -95,7 +95,7 @@ struct TileLayout {
   static constexpr int kNB = align16(kTM + 3 * NFQ * NE * 8);    // int4 [E]
   static constexpr int kEL = align16(kNB + E * 16);              // int [E] global element index
   static constexpr int kItems = align16(kEL + E * 4);            // int [kMaxItems]
-  static constexpr int kBar = align16(kItems + kMaxItems * 4);   // mbarrier (8 B) + abort flag
+  static constexpr int kBar = align16(kItems + kMaxItems * 4);   // mbarrier (8 B), abort flag, face count
   static constexpr int kRuns = kBar + 16;                        // int4 [2] tile descriptor, one copy per run
   static constexpr int kBytes = align16(kRuns + 32);
 };
@@ -388,6 +388,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
   int* items = reinterpret_cast<int*>(smem + L::kItems);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + L::kBar);
   int* abort_flag = reinterpret_cast<int*>(smem + L::kBar + 8);
+  int* NITEMS = reinterpret_cast<int*>(smem + L::kBar + 12);  // the tile's face count
   int4* RUNS = reinterpret_cast<int4*>(smem + L::kRuns);
 
   const int t = threadIdx.x;
@@ -412,7 +413,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
   // its state copies
   int tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  int nitems = __ldg(a.tile_count + tile);
+  if (t == 0) *NITEMS = __ldg(a.tile_count + tile);
   {
     const int4 run = __ldg(a.tiles + tile);
     if (lane == 0 && t < 64) RUNS[t >> 5] = run;
@@ -506,6 +507,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     if (*abort_flag) break;
 
     // ---- 3. faces: the flux overwrites the traces it consumed ----------------------------
+    const int nitems = *NITEMS;
     for (int w = t; w < nitems * NFQ; w += T) {
       const int it = items[w / NFQ];
       const int q = w % NFQ;
@@ -583,8 +585,8 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     // below and at the next tile's start).
     if (lane == 0 && t < 64) RUNS[t >> 5] = next_run;
     if (has_next) {
-      nitems = __ldg(a.tile_count + tile + G);
       if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t);
+      if (t == kMaxItems) cp_async4(NITEMS, a.tile_count + tile + G);
       if (grp == 0) {
         const int pos = col % kTileRun;
         const bool second = col >= kTileRun;
