@@ -97,7 +97,8 @@ struct TileLayout {
   static constexpr int kItems = align16(kEL + E * 4);            // int [kMaxItems]
   static constexpr int kBar = align16(kItems + kMaxItems * 4);   // mbarrier (8 B), abort flag, face count
   static constexpr int kRuns = kBar + 16;                        // int4 [2] tile descriptor, one copy per run
-  static constexpr int kBytes = align16(kRuns + 32);
+  static constexpr int kNext = kRuns + 32;                       // int4 [2] next tile's descriptor, per run
+  static constexpr int kBytes = align16(kNext + 32);
 };
 
 // ---- TMA unit ------------------------------------------------------------------
@@ -390,6 +391,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
   int* abort_flag = reinterpret_cast<int*>(smem + L::kBar + 8);
   int* NITEMS = reinterpret_cast<int*>(smem + L::kBar + 12);  // the tile's face count
   int4* RUNS = reinterpret_cast<int4*>(smem + L::kRuns);
+  int4* NEXT = reinterpret_cast<int4*>(smem + L::kNext);
 
   const int t = threadIdx.x;
   const int col = t % E, grp = t / E;  // load mapping; also (element, group) later
@@ -464,8 +466,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     }
 
     // ---- 1. load ------------------------------------------------------------------
-    int4 next_run = make_int4(0, 0, 0, 0);
-    if (has_next) next_run = __ldg(a.tiles + tile + G);
+    // the next tile's descriptor, by cp.async into the run's own slot (lane 0
+    // of warp 0 or 1 issues, waits before the barrier after the traces and
+    // copies it into RUNS after the faces), so no register holds it across the
+    // trace and face phases
+    if (lane == 0 && t < 64 && has_next) cp_async16(NEXT + (t >> 5), a.tiles + tile + G);
     {
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
@@ -577,22 +582,16 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
     }
     __syncthreads();
 
-    // next tile's metadata (next_run has arrived by now). The face list,
-    // neighbour table and element indices of this tile are no longer read, so
-    // the next tile's go to shared memory now; the item rows are kMaxItems
-    // wide, so the copy need not wait for the item count. The descriptor
-    // copies are read again after this run's next barrier (by the copy issue
-    // below and at the next tile's start).
-    if (lane == 0 && t < 64) RUNS[t >> 5] = next_run;
+    // next tile's metadata. The face list and face count of this tile are no
+    // longer read, so the next tile's go to shared memory now (the item rows
+    // are kMaxItems wide, so the copy need not wait for the item count), and
+    // the next descriptor into RUNS; the descriptor copies are read again
+    // after this run's next barrier (the neighbour table's copy below, the
+    // copy issue after the nodal flux, and the next tile's start).
+    if (lane == 0 && t < 64) RUNS[t >> 5] = has_next ? NEXT[t >> 5] : make_int4(0, 0, 0, 0);
     if (has_next) {
       if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t);
       if (t == kMaxItems) cp_async4(NITEMS, a.tile_count + tile + G);
-      if (grp == 0) {
-        const int pos = col % kTileRun;
-        const bool second = col >= kTileRun;
-        if (pos < (second ? next_run.w : next_run.y)) cp_async16(NB + col, a.nbr + (second ? next_run.z : next_run.x) + pos);
-        else NB[col] = make_int4(0, 0, 0, 0);
-      }
     }
 
     // ---- 4. lift ---------------------------------------------------------------------------
@@ -629,10 +628,16 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
       }
     }
     (void)NR;
-    // the next tile's neighbour table has landed (its copies were issued before
-    // the lift); the run's barrier makes it visible to the column's other threads
-    if (grp == 0) cp_async_wait_all();
     run_sync(t);
+
+    // the next tile's neighbour table, now that the run's barrier has made its
+    // descriptor visible; it lands during the nodal flux phase
+    if (has_next && grp == 0) {
+      const int4 nr = RUNS[col >= kTileRun];
+      const int pos = col % kTileRun;
+      if (pos < (col >= kTileRun ? nr.w : nr.y)) cp_async16(NB + col, a.nbr + (col >= kTileRun ? nr.z : nr.x) + pos);
+      else NB[col] = make_int4(0, 0, 0, 0);
+    }
 
     // ---- 5. nodal flux of every node, once, contracted with the inverse Jacobian --------
     if (P > 0) {
@@ -657,6 +662,8 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
         }
       }
     }
+    // the neighbour table has landed; the barrier shows it to the column's other threads
+    if (grp == 0) cp_async_wait_all();
     run_sync(t);
 
     // this run's columns of the state tile are free: start its next copies and neighbour rows
