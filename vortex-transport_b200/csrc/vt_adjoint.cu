@@ -72,7 +72,12 @@ cudaError_t launch_tile(const AdjArgs& a, const double* ops, int max_blocks, cud
   StageOps<P, NFQ> o;
   std::memcpy(&o, ops, sizeof(o));
   const int grid = a.ntiles < max_blocks ? a.ntiles : max_blocks;
-  adjoint_tile_kernel<P, NFQ><<<grid, 4 * kTileElems, AdjTileLayout<P, NFQ>::kBytes, st>>>(a, o);
+  // the tensor maps of this launch's stage state and stage adjoint (host-side encoding, no allocation)
+  AdjArgs k = a;
+  cudaError_t e = encode_state_map(&k.map_U, a.U, a.Kpad, np_of_p(P));
+  if (!e) e = encode_state_map(&k.map_a, a.a, a.Kpad, np_of_p(P));
+  if (e) return e;
+  adjoint_tile_kernel<P, NFQ><<<grid, 4 * kTileElems, AdjTileLayout<P, NFQ>::kBytes, st>>>(k, o);
   return cudaGetLastError();
 }
 

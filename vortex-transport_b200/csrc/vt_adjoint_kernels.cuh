@@ -56,6 +56,10 @@ struct AdjArgs {
   long long Kpad;
   int K;
   double sa, lam_coef, cl, cg;
+  // 2-D tensor maps of U and a (adjoint_tile_kernel only), as the stage
+  // kernel's: [2 Np rows] x [2 Kpad doubles], a box of one 32-element run;
+  // encoded on the host by the launcher
+  CUtensorMap map_U, map_a;
 };
 
 constexpr int kAdjRun = 32;  // elements per block (one per lane)

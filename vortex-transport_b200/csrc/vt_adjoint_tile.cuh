@@ -9,8 +9,10 @@
 // intermediate in shared memory, so nothing but the state, the adjoints and
 // the geometry crosses HBM:
 //
-//   1. load   the tile's stage-state rows by TMA bulk copies (issued during the
-//             previous tile), the side-0 neighbours' side nodes, the face list;
+//   1. load   the tile's stage state and stage adjoint by one 2-D TMA tensor
+//             copy each per run (issued during the previous tile); the
+//             side-0 neighbours' side nodes, the neighbour table and the face
+//             list by cp.async during the previous tile;
 //   2. lift^T thread (element, component): the lifted face adjoint
 //             bF(s, q) = -(len_s/detJ) sa sum_i LIFT_s[i][q] a_i at every face
 //             point (the transpose of the lift and of the folded mass inverse);
@@ -32,8 +34,8 @@
 // As in the stage kernel, from phase 4 on every shared-memory access stays
 // within an element's four threads, so the barriers after phases 4a, 4b and 5
 // are per-run named barriers and each run issues its own next copies; the load
-// phase has no block barrier (phase 2 reads only global memory and writes the
-// thread's own column, phase 3 comes after a barrier), and a tile ends with a
+// phase has no block barrier (phase 2 reads and writes only the thread's own
+// column, phase 3 comes after a barrier), and a tile ends with a
 // per-run barrier (the next tile's phase 2 reuses rows that this tile's phase
 // 6 reads in other warps of the same run).
 //
@@ -48,7 +50,9 @@
 namespace vt {
 
 // The stage kernel's shared-memory layout plus the two operator tables the
-// face phase indexes at run time (side and face point differ across a warp).
+// face phase indexes at run time (side and face point differ across a warp)
+// and the stage adjoint tile, which arrives by tensor copy like the state
+// tile (both [2 runs][2 Np rows][32 elements] of double2, 128-byte aligned).
 template <int P, int NFQ>
 struct AdjTileLayout {
   using Base = TileLayout<P, NFQ>;
@@ -56,7 +60,8 @@ struct AdjTileLayout {
   static constexpr int NE = Base::NE;
   static constexpr int kTP = align16(Base::kBytes);            // double [3][NFQ][NE] own trace weights
   static constexpr int kLF = align16(kTP + 3 * NFQ * NE * 8);  // double [3][NP][NFQ] LIFT
-  static constexpr int kBytes = align16(kLF + 3 * NP * NFQ * 8);
+  static constexpr int kA = (kLF + 3 * NP * NFQ * 8 + 127) / 128 * 128;  // double2 [2][2NP][32] stage adjoint
+  static constexpr int kBytes = kA + 2 * 2 * NP * kTileRun * 16;
 };
 
 // component c of node i of an SoA double2 state, element e
@@ -64,11 +69,33 @@ __device__ __forceinline__ long long comp_index(long long KP, int i, int c, int 
   return ((2 * i + (c >> 1)) * KP + e) * 2 + (c & 1);
 }
 
+// Lane 0 of warp `which` announces its run's two boxes (stage state and stage
+// adjoint) on the tile's mbarrier and issues both tensor copies.
+template <int NP>
+__device__ __forceinline__ void issue_adj_run_copies(const AdjArgs& a, const int4 run, int which, double2* S,
+                                                     double2* A, unsigned long long* bar, int lane) {
+  if (lane != 0) return;
+  const int start = which ? run.z : run.x, len = which ? run.w : run.y;
+  fence_proxy_async_smem();
+  mbar_arrive_expect_tx(bar, len > 0 ? 2u * 2u * NP * kTileRun * 16u : 0u);
+  if (len > 0) {
+    tensor_g2s(S + which * 2 * NP * kTileRun, &a.map_U, 2 * start, 0, bar);
+    tensor_g2s(A + which * 2 * NP * kTileRun, &a.map_a, 2 * start, 0, bar);
+  }
+}
+
 // Two 256-thread blocks per SM: the transposed Roe Jacobian needs about 128
 // registers per thread; capped at 80 (three blocks) it spills 416 bytes and the
-// reverse stage runs 18% slower.
+// reverse stage runs 18% slower. Two blocks leave shared memory for the stage
+// adjoint tile (about 96 KB per block at p = 3).
+//
+// Loads follow the stage kernel: the tile's stage state and stage adjoint
+// arrive by one 2-D tensor copy each per run, issued when that run finished
+// the previous tile's transposed nodal flux; the next tile's descriptor, face
+// list, face count, neighbour table and side-0 neighbour rows go straight to
+// shared memory by cp.async, so no register holds them across a tile.
 template <int P, int NFQ>
-__global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const AdjArgs a,
+__global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const __grid_constant__ AdjArgs a,
                                                                           const StageOps<P, NFQ> ops) {
   using B = TileLayout<P, NFQ>;
   using L = AdjTileLayout<P, NFQ>;
@@ -78,7 +105,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
   constexpr int ES = B::ES;
   constexpr int T = 4 * E;
   extern __shared__ __align__(128) unsigned char smem[];
-  double2* S = reinterpret_cast<double2*>(smem + B::kS);
+  double2* S = reinterpret_cast<double2*>(smem + B::kS);  // stage state tile, sidx layout
   double2* H = reinterpret_cast<double2*>(smem + B::kH);
   double* FB = reinterpret_cast<double*>(smem + B::kFB);
   double* TM = reinterpret_cast<double*>(smem + B::kTM);
@@ -87,15 +114,19 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
   int* items = reinterpret_cast<int*>(smem + B::kItems);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + B::kBar);
   int* abort_flag = reinterpret_cast<int*>(smem + B::kBar + 8);
+  int* NITEMS = reinterpret_cast<int*>(smem + B::kBar + 12);  // the tile's face count
+  int4* RUNS = reinterpret_cast<int4*>(smem + B::kRuns);      // tile descriptor, one copy per run
+  int4* NEXT = reinterpret_cast<int4*>(smem + B::kNext);      // next tile's descriptor, per run
   double* TP = reinterpret_cast<double*>(smem + L::kTP);
   double* LF = reinterpret_cast<double*>(smem + L::kLF);
+  double2* A = reinterpret_cast<double2*>(smem + L::kA);  // stage adjoint tile, sidx layout
+  const double* Ad = reinterpret_cast<const double*>(A);
 
   const int t = threadIdx.x;
   const int col = t % E, grp = t / E;
   const int lane = t & 31;
   const long long KP = a.Kpad;
   const int G = gridDim.x;
-  const double* Ad = reinterpret_cast<const double*>(a.a);
 
   {
     const double* tm = &ops.tm[0][0][0];
@@ -113,48 +144,56 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
   }
   __syncthreads();
 
+  // the first tile: descriptor, face count, and by cp.async its face list,
+  // neighbour table and side-0 neighbour rows; then its tensor copies
   int tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  int4 run = __ldg(a.tiles + tile);
-  int nitems = __ldg(a.tile_count + tile);
-  int my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile) * kMaxItems + t) : 0;
-  int4 my_nb = make_int4(0, 0, 0, 0);
-  double2 hreg[2];
+  if (t == 0) *NITEMS = __ldg(a.tile_count + tile);
   {
+    const int4 run = __ldg(a.tiles + tile);
+    if (lane == 0 && t < 64) RUNS[t >> 5] = run;
     const int pos = col % kTileRun;
     const bool second = col >= kTileRun;
     const bool valid = pos < (second ? run.w : run.y);
-    if (valid) my_nb = __ldg(a.nbr + (second ? run.z : run.x) + pos);
+    const int4* nsrc = a.nbr + (second ? run.z : run.x) + pos;
+    const int nbx = valid ? __ldg(&nsrc->x) : 0;
+    if (grp == 0) {
+      if (valid) cp_async16(NB + col, nsrc);
+      else NB[col] = make_int4(0, 0, 0, 0);
+    }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int r = grp + 4 * k;
-      hreg[k] = (valid && r < 2 * NE) ? __ldg(a.U + r * KP + my_nb.x) : make_double2(1.0, 0.0);
+      if (r < 2 * NE) {
+        if (valid) cp_async16(H + r * ES + col, a.U + r * KP + nbx);
+        else H[r * ES + col] = make_double2(1.0, 0.0);
+      }
     }
+    if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile) * kMaxItems + t);
+    cp_async_commit();
+    if (t < 64) issue_adj_run_copies<NP>(a, run, t >> 5, S, A, bar, lane);
   }
-  if (t < 64) issue_run_copies<NP, ES>(a.U, KP, run, t >> 5, S, bar, lane);
+  __syncthreads();
   unsigned parity = 0;
 
   for (; tile < a.ntiles; tile += G) {
     const bool has_next = tile + G < a.ntiles;
 
     // ---- 1. load ------------------------------------------------------------------
-    int4 next_run = make_int4(0, 0, 0, 0);
-    if (has_next) next_run = __ldg(a.tiles + tile + G);
+    // the next tile's descriptor, by cp.async into the run's own slot (waited
+    // for before the barrier after phase 2, copied into RUNS after the faces)
+    if (lane == 0 && t < 64 && has_next) cp_async16(NEXT + (t >> 5), a.tiles + tile + G);
+    const int c = grp;  // uniform per warp
+    const int el = col;
+    int e;
     {
+      const int4 run = RUNS[(t >> 5) & 1];
       const int pos = col % kTileRun;
       const bool second = col >= kTileRun;
-      const bool valid = pos < (second ? run.w : run.y);
-      if (grp == 0) {
-        NB[col] = my_nb;
-        EL[col] = valid ? (second ? run.z : run.x) + pos : -1;
-      }
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int r = grp + 4 * k;
-        if (r < 2 * NE) H[r * ES + col] = hreg[k];
-      }
-      if (t < nitems) items[t] = my_item;
+      e = pos < (second ? run.w : run.y) ? (second ? run.z : run.x) + pos : -1;
+      if (grp == 0) EL[col] = e;
     }
+    const bool valid = e >= 0;
     {
       bool ok = false;
       for (unsigned n = 0; n < kMaxWaitTries && !ok; ++n) ok = mbar_try_wait(bar, parity);
@@ -166,16 +205,12 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
     parity ^= 1u;
 
     // ---- 2. lifted face adjoints bF[s][c][q][el], thread (element el, component c) ----
-    const int c = grp;  // uniform per warp
-    const int el = col;
-    const bool valid = col % kTileRun < (col >= kTileRun ? run.w : run.y);
-    const int e = valid ? (col >= kTileRun ? run.z : run.x) + col % kTileRun : -1;  // EL[el]
     const double sa = valid && a.elem_dt && a.sa_dt ? a.sa * __ldg(a.elem_dt + e) : a.sa;
     {
       double lam[NP];
       double2 lsa = make_double2(0.0, 0.0), lsb = lsa;
 #pragma unroll
-      for (int i = 0; i < NP; ++i) lam[i] = valid ? __ldg(Ad + comp_index(KP, i, c, e)) : 0.0;
+      for (int i = 0; i < NP; ++i) lam[i] = valid ? Ad[sidx<NP>(2 * i + (c >> 1), el) * 2 + (c & 1)] : 0.0;
       if (valid) {
         lsa = __ldg(a.geo + 5 * KP + e);
         lsb = __ldg(a.geo + 6 * KP + e);
@@ -192,10 +227,12 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
         }
       }
     }
+    cp_async_wait_all();  // this thread's cp.async copies of the tile's face list and neighbour rows
     __syncthreads();
     if (*abort_flag) break;
 
     // ---- 3. faces: transposed Roe Jacobian; the trace adjoints overwrite bF ----------
+    const int nitems = *NITEMS;
     for (int w = t; w < nitems * NFQ; w += T) {
       const int it = items[w / NFQ];
       const int q = w % NFQ;
@@ -210,7 +247,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       for (int k = 0; k < NE; ++k) {
         const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
         const double cp = TP[(s * NFQ + q) * NE + k];
-        const double2 x0 = S[(2 * node) * ES + fl], x1 = S[(2 * node + 1) * ES + fl];
+        const double2 x0 = S[sidx<NP>(2 * node, fl)], x1 = S[sidx<NP>(2 * node + 1, fl)];
         up[0] = fma(cp, x0.x, up[0]);
         up[1] = fma(cp, x0.y, up[1]);
         up[2] = fma(cp, x1.x, up[2]);
@@ -222,7 +259,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
         for (int k = 0; k < NE; ++k) {
           const int node = s == 0 ? edge_node(P, 0, k) : (s == 1 ? edge_node(P, 1, k) : edge_node(P, 2, k));
           const double cm = TP[(s * NFQ + qm) * NE + k];
-          const double2 y0 = S[(2 * node) * ES + nl], y1 = S[(2 * node + 1) * ES + nl];
+          const double2 y0 = S[sidx<NP>(2 * node, nl)], y1 = S[sidx<NP>(2 * node + 1, nl)];
           um[0] = fma(cm, y0.x, um[0]);
           um[1] = fma(cm, y0.y, um[1]);
           um[2] = fma(cm, y1.x, um[2]);
@@ -280,14 +317,13 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
     }
     __syncthreads();
 
-    // next tile's metadata (next_run has arrived by now)
+    // next tile's metadata: the face list and count of this tile are no longer
+    // read, so the next tile's go to shared memory now, and the next
+    // descriptor into RUNS (read again after this run's next barrier)
+    if (lane == 0 && t < 64) RUNS[t >> 5] = has_next ? NEXT[t >> 5] : make_int4(0, 0, 0, 0);
     if (has_next) {
-      nitems = __ldg(a.tile_count + tile + G);
-      my_item = t < nitems ? __ldg(a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t) : 0;
-      const int pos = col % kTileRun;
-      const bool second = col >= kTileRun;
-      my_nb = pos < (second ? next_run.w : next_run.y) ? __ldg(a.nbr + (second ? next_run.z : next_run.x) + pos)
-                                                       : make_int4(0, 0, 0, 0);
+      if (t < kMaxItems) cp_async4(items + t, a.tile_items + static_cast<long long>(tile + G) * kMaxItems + t);
+      if (t == kMaxItems) cp_async4(NITEMS, a.tile_count + tile + G);
     }
 
     // ---- 4a. trace adjoints onto the side nodes, component c --------------------------
@@ -304,12 +340,21 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
       }
     run_sync(t);
 
+    // the next tile's neighbour table, now that the run's barrier has made its
+    // descriptor visible; it lands during phases 4b and 5
+    if (has_next && grp == 0) {
+      const int4 nr = RUNS[col >= kTileRun];
+      const int pos = col % kTileRun;
+      if (pos < (col >= kTileRun ? nr.w : nr.y)) cp_async16(NB + col, a.nbr + (col >= kTileRun ? nr.z : nr.x) + pos);
+      else NB[col] = make_int4(0, 0, 0, 0);
+    }
+
     // ---- 4b. transposed volume operator: rows j*8 + c (xi), j*8 + 4 + c (eta) ---------
     double* Gs = FB;
     if (P > 0) {
       double lam[NP];
 #pragma unroll
-      for (int i = 0; i < NP; ++i) lam[i] = valid ? __ldg(Ad + comp_index(KP, i, c, e)) : 0.0;
+      for (int i = 0; i < NP; ++i) lam[i] = valid ? Ad[sidx<NP>(2 * i + (c >> 1), el) * 2 + (c & 1)] : 0.0;
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         double bx = 0.0, by = 0.0;
@@ -326,11 +371,11 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
 
     // ---- 5. transposed nodal flux Jacobian of every node, in place over the xi rows ----
     if (P > 0) {
-      const int eg = valid ? e : run.x;
+      const int eg = valid ? e : 0;
       const double2 j0 = __ldg(a.geo + 0 * KP + eg);
       const double2 j1 = __ldg(a.geo + 1 * KP + eg);
       for (int j = c; j < NP; j += 4) {
-        const double2 s0 = S[(2 * j) * ES + el], s1 = S[(2 * j + 1) * ES + el];
+        const double2 s0 = S[sidx<NP>(2 * j, el)], s1 = S[sidx<NP>(2 * j + 1, el)];
         const double sv[4] = {s0.x, s0.y, s1.x, s1.y};
         double bx[4], by[4], gv[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -343,20 +388,27 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
         for (int cc = 0; cc < 4; ++cc) Gs[(j * 8 + cc) * ES + el] = gv[cc];
       }
     }
+    // the neighbour table has landed; the barrier shows it to the column's other threads
+    if (grp == 0) cp_async_wait_all();
     run_sync(t);
 
-    // this run's columns of the state tile are free: start its next copies and neighbour rows
+    // this run's columns of the state and adjoint tiles are free: start its
+    // next copies and the next tile's side-0 neighbour rows
     if (has_next) {
-      if (t < 64) issue_run_copies<NP, ES>(a.U, KP, next_run, t >> 5, S, bar, lane);
-      const int pos = col % kTileRun;
-      const bool second = col >= kTileRun;
-      const bool nvalid = pos < (second ? next_run.w : next_run.y);
+      if (t < 64) issue_adj_run_copies<NP>(a, RUNS[t >> 5], t >> 5, S, A, bar, lane);
+      const int4 nr = RUNS[col >= kTileRun];
+      const bool nvalid = col % kTileRun < (col >= kTileRun ? nr.w : nr.y);
+      const int nbx = NB[col].x;
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const int rr = grp + 4 * k;
-        hreg[k] = (nvalid && rr < 2 * NE) ? __ldg(a.U + rr * KP + my_nb.x) : make_double2(1.0, 0.0);
+        if (rr < 2 * NE) {
+          if (nvalid) cp_async16(H + rr * ES + col, a.U + rr * KP + nbx);
+          else H[rr * ES + col] = make_double2(1.0, 0.0);
+        }
       }
     }
+    cp_async_commit();
 
     // ---- 6. reverse RK combine, component c of every node ------------------------------
     if (valid) {
@@ -386,13 +438,13 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const A
         if (aout) aout[x] = fma(cl, lv[i], cg * gi);
       }
     }
-    run = next_run;
     // the four warps of a run hold different components of the same elements:
-    // none may start the next tile's traces (which reuse rows of the face /
+    // none may start the next tile's phase 2 (which reuses rows of the face /
     // flux buffer) before the others are done with this tile's
     run_sync(t);
   }
 
+  cp_async_wait_all();  // none may land after the block has left
   if (*abort_flag) {
     // the bulk copies of a tile whose wait gave up may still land: wait for
     // them once more, with the same bound, before the block leaves

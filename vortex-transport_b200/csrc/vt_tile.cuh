@@ -102,11 +102,6 @@ struct TileLayout {
 };
 
 // ---- TMA unit ------------------------------------------------------------------
-// L2 prefetch of [p, p + bytes) (bytes a multiple of 16, p 16-byte aligned).
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
@@ -136,16 +131,6 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
   return ok != 0;
 }
 
-// Bulk copy of `bytes` (multiple of 16, both ends 16-byte aligned) from global
-// to this CTA's shared memory, completing on `bar`.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-
 // Global-to-shared copies that bypass the registers (cp.async, completed per
 // thread by cp.async.wait_all): 16 bytes (both addresses 16-byte aligned,
 // cached in L2 only) or 4 bytes.
@@ -165,25 +150,6 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 constexpr unsigned kMaxWaitTries = 1u << 22;
-
-// Warp `which` (0 or 1) issues the bulk copies of its run's 2*Np state rows
-// into columns which*32.. of S, after lane 0 announced the run's byte count on
-// the barrier (which expects one arrival per run).
-template <int NP, int ES>
-__device__ __forceinline__ void issue_run_copies(const double2* src, long long Kpad, const int4 run, int which,
-                                                 double2* S, unsigned long long* bar, int lane, int test_flags = 0) {
-  if (test_flags & kTestNoCopies) return;  // test hook: nothing arrives, every wait gives up
-  const int start = which ? run.z : run.x;
-  const unsigned bytes = static_cast<unsigned>(which ? run.w : run.y) * 16u;
-  if (lane == 0) {
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(bar, 2u * NP * bytes);
-  }
-  __syncwarp();
-  if (bytes)
-    for (int r = lane; r < 2 * NP; r += 32) bulk_g2s(S + r * ES + which * kTileRun, src + r * Kpad + start, bytes, bar);
-}
-
 
 // Shared-memory index of (row, element column) of the state tile: each run's
 // tensor box lands dense, [2 Np rows][32 elements] per run.
