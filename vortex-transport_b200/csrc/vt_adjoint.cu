@@ -291,8 +291,10 @@ double2* slot(vt_ctx* c, long long i) {
 }
 
 cudaError_t stage(vt_ctx* c, const double2* in, const double2* base, double2* out, int st, double ca, double co,
-                  cudaStream_t stream) {
-  return c->launch(stage_args(c, in, base, c->A, out, st, ca, co), c->ops.data(), c->max_blocks, stream);
+                  cudaStream_t stream, bool no_acc = false) {
+  StageArgs a = stage_args(c, in, base, c->A, out, st, ca, co);
+  a.no_acc = no_acc ? 1 : 0;
+  return c->launch(a, c->ops.data(), c->max_blocks, stream);
 }
 
 // The step size the coefficients carry: dt, or 1 when the device scales them
@@ -316,19 +318,21 @@ cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt, c
 }
 
 // Step from X keeping the stage states in S1, S2, S3; the new state goes to
-// `out` when given (else the last stage is not run).
+// `out` when given (else the last stage is not run). With no_acc (only when
+// no last stage will follow on this accumulator: the reverse sweeps' reruns)
+// stages 0-2 neither read nor write the accumulator.
 cudaError_t stage_step(vt_ctx* c, const double2* X, double2* S1, double2* S2, double2* S3, double dt0,
-                       double2* out, cudaStream_t st) {
+                       double2* out, cudaStream_t st, bool no_acc = false) {
   const double dt = dt_scale(c, dt0);
   cudaError_t e;
-  if ((e = stage(c, X, X, S1, 0, (1.0 / 6) * dt, 0.5 * dt, st))) return e;
-  if ((e = stage(c, S1, X, S2, 1, (1.0 / 3) * dt, 0.5 * dt, st))) return e;
-  if ((e = stage(c, S2, X, S3, 2, (1.0 / 3) * dt, dt, st))) return e;
+  if ((e = stage(c, X, X, S1, 0, (1.0 / 6) * dt, 0.5 * dt, st, no_acc))) return e;
+  if ((e = stage(c, S1, X, S2, 1, (1.0 / 3) * dt, 0.5 * dt, st, no_acc))) return e;
+  if ((e = stage(c, S2, X, S3, 2, (1.0 / 3) * dt, dt, st, no_acc))) return e;
   return out ? stage(c, S3, X, out, 3, 0.0, (1.0 / 6) * dt, st) : cudaSuccess;
 }
 
-cudaError_t stage_step(vt_ctx* c, const double2* X, double dt, double2* out) {
-  return stage_step(c, X, c->adj->s1, c->adj->s2, c->adj->s3, dt, out, c->stream);
+cudaError_t stage_step(vt_ctx* c, const double2* X, double dt, double2* out, bool no_acc = false) {
+  return stage_step(c, X, c->adj->s1, c->adj->s2, c->adj->s3, dt, out, c->stream, no_acc);
 }
 
 AdjArgs adj_args(vt_ctx* c) {
@@ -387,9 +391,13 @@ cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
     const CkptAction& a = s->plan[i];
     switch (a.op) {
       case CkptOp::kAdvance: e = advance(c, slot(c, a.src), a.steps, slot(c, a.dst), s->dt, c->stream); break;
-      case CkptOp::kStageStep:
-        e = stage_step(c, slot(c, a.src), s->dt, a.step == s->nsteps - 1 ? out_last : nullptr);
+      case CkptOp::kStageStep: {
+        // the forward sweep's last step runs its last stage into out_last;
+        // every other rerun only keeps its stage states
+        double2* out = a.step == s->nsteps - 1 ? out_last : nullptr;
+        e = stage_step(c, slot(c, a.src), s->dt, out, out == nullptr);
         break;
+      }
       case CkptOp::kAdjoint: e = adjoint_step(c, slot(c, a.src), s->s1, s->s2, s->s3, s->dt); break;
     }
   }
@@ -433,7 +441,7 @@ cudaError_t run_plan_overlapped(vt_ctx* c, size_t begin, size_t end) {
       case CkptOp::kStageStep: {
         const int w = cur ^ 1;
         if (freed_rec[w]) e = cudaStreamWaitEvent(R, s->ev_freed[w], 0);
-        if (!e) e = stage_step(c, slot(c, a.src), sets[w][0], sets[w][1], sets[w][2], s->dt, nullptr, R);
+        if (!e) e = stage_step(c, slot(c, a.src), sets[w][0], sets[w][1], sets[w][2], s->dt, nullptr, R, true);
         if (!e) e = cudaEventRecord(s->ev_ready[w], R);
         ready_rec[w] = true;
         cur = w;

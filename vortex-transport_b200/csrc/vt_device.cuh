@@ -81,6 +81,9 @@ struct StageArgs {
   // test_flags issues no state copies at all, so every wait gives up.
   unsigned wait_tries = 0;
   int test_flags = 0;
+  // RK4 stages 0-2 that only produce the next stage state (a step rerun to
+  // keep its stage states): the accumulator is neither read nor written
+  int no_acc = 0;
   // 2-D tensor maps of in / acc / base, [2 Np rows] x [2 Kpad doubles], box of
   // 2 Np rows x 64 doubles (one 32-element run); encoded on the host by the
   // launcher, read by the tensor copies through this grid-constant parameter

@@ -299,14 +299,20 @@ __device__ __forceinline__ void pair_update(const StageArgs& a, int e, int h, do
   constexpr int N = NP - HALF * NH < NH ? NP - HALF * NH : NH;  // nodes of this half
   switch (a.stage) {
     case 0:
+      if (!a.no_acc) {
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
-        a.acc[o + i * 2 * KP] = fma2(c_acc, r[i], pre[i]);
-        a.out[o + i * 2 * KP] = fma2(c_out, r[i], pre[i]);
+        for (int i = 0; i < N; ++i) a.acc[o + i * 2 * KP] = fma2(c_acc, r[i], pre[i]);
       }
+#pragma unroll
+      for (int i = 0; i < N; ++i) a.out[o + i * 2 * KP] = fma2(c_out, r[i], pre[i]);
       break;
     case 1:
     case 2: {
+      if (a.no_acc) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) a.out[o + i * 2 * KP] = fma2(c_out, r[i], pre[i]);
+        break;
+      }
       // every accumulator row is read before the first store: a load that
       // follows a store to another array cannot be moved above it, so read
       // and written in turn each row would wait on its own memory round trip
@@ -421,7 +427,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
       const int which = t & 1, vec = (t - 64) >> 1;  // vec 0: acc, 1: base
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
       if (len > 0) {
-        if (vec == 0 && a.stage >= 1 && a.stage <= 3) tensor_prefetch_l2(&a.map_acc, 2 * start, 0);
+        if (vec == 0 && a.stage >= 1 && a.stage <= 3 && !a.no_acc) tensor_prefetch_l2(&a.map_acc, 2 * start, 0);
         if (vec == 1 && (a.stage == 1 || a.stage == 2)) tensor_prefetch_l2(&a.map_base, 2 * start, 0);
       }
     } else if (t >= 64 + 8 * NP && t < 64 + 8 * NP + 56) {
@@ -703,14 +709,20 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
         const long long step = 4 * KP;  // doubles between node rows of the same pair
         switch (a.stage) {
           case 0:
+            if (!a.no_acc) {
 #pragma unroll
-            for (int i = 0; i < NP; ++i) {
-              acc[i * step] = fma(c_acc, r[i], pre[i]);
-              out[i * step] = fma(c_out, r[i], pre[i]);
+              for (int i = 0; i < NP; ++i) acc[i * step] = fma(c_acc, r[i], pre[i]);
             }
+#pragma unroll
+            for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], pre[i]);
             break;
           case 1:
           case 2: {
+            if (a.no_acc) {
+#pragma unroll
+              for (int i = 0; i < NP; ++i) out[i * step] = fma(c_out, r[i], pre[i]);
+              break;
+            }
             double av[NP];  // all reads before the first store, as in pair_update
 #pragma unroll
             for (int i = 0; i < NP; ++i) av[i] = acc[i * step];
