@@ -146,6 +146,13 @@ struct SweepGraph {
   }
 };
 
+// The overlapped reverse sweep (run_plan_overlapped) renames the checkpoint
+// slots onto the plan's slots, the work slot and kSpareSlots spare state
+// buffers, and orders its two streams through a ring of kRevRing events, one
+// recorded after each reverse step.
+constexpr int kSpareSlots = 2;
+constexpr int kRevRing = 8;
+
 struct AdjointState {
   AdjKernels k;
   SweepGraph fwd_graph, bwd_graph;
@@ -159,7 +166,8 @@ struct AdjointState {
   // the reverse sweep's recomputation runs on `side`, ahead of the reverse
   // steps on the context's stream (run_plan_overlapped)
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ready[2] = {nullptr, nullptr}, ev_freed[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ready[2] = {nullptr, nullptr};
+  cudaEvent_t ev_rev[kRevRing] = {};
   double2 *bp = nullptr, *bm = nullptr;  // face adjoints of the two-launch form (else null)
   // fused reverse stage (adjoint_tile_kernel): persistent grid size, 0 when
   // the edge-once form does not apply (the element adjacency does not
@@ -167,6 +175,7 @@ struct AdjointState {
   int tile_blocks = 0;
   double2* slots = nullptr;
   long long nslots = 0;
+  int plan_slots = 0;  // checkpoint slots the plan uses (the spares follow them)
   // last forward sweep
   std::vector<CkptAction> plan;
   size_t first_adjoint = 0;
@@ -181,8 +190,10 @@ struct AdjointState {
 namespace {
 
 void release_streams(AdjointState* s) {
-  cudaEvent_t evs[6] = {s->ev_fork, s->ev_join, s->ev_ready[0], s->ev_ready[1], s->ev_freed[0], s->ev_freed[1]};
+  cudaEvent_t evs[4] = {s->ev_fork, s->ev_join, s->ev_ready[0], s->ev_ready[1]};
   for (cudaEvent_t ev : evs)
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : s->ev_rev)
     if (ev) cudaEventDestroy(ev);
   if (s->side) cudaStreamDestroy(s->side);
   s->side = nullptr;
@@ -246,8 +257,9 @@ int setup(vt_ctx* c) {
   }
   auto* s = new AdjointState();
   e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
-  cudaEvent_t* evs[6] = {&s->ev_fork, &s->ev_join, &s->ev_ready[0], &s->ev_ready[1], &s->ev_freed[0], &s->ev_freed[1]};
-  for (int i = 0; i < 6 && !e; ++i) e = cudaEventCreateWithFlags(evs[i], cudaEventDisableTiming);
+  cudaEvent_t* evs[4 + kRevRing] = {&s->ev_fork, &s->ev_join, &s->ev_ready[0], &s->ev_ready[1]};
+  for (int i = 0; i < kRevRing; ++i) evs[4 + i] = &s->ev_rev[i];
+  for (int i = 0; i < 4 + kRevRing && !e; ++i) e = cudaEventCreateWithFlags(evs[i], cudaEventDisableTiming);
   if (e) {
     cudaGetLastError();
     release_streams(s);
@@ -404,57 +416,100 @@ cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
   return e;
 }
 
-// Runs plan[begin, end) of a reverse sweep with the recomputation one step
-// ahead: advances and stage steps go to the side stream, reverse steps stay on
-// the context's stream, and the stage states alternate between two sets, so
-// that the recomputation of step i-1 overlaps the reverse of step i (at small
+// Runs plan[begin, end) of a reverse sweep with the recomputation ahead of it:
+// advances and stage steps go to the side stream R, reverse steps stay on the
+// context's stream M, and the stage states alternate between two sets, so that
+// the recomputation of the next steps overlaps the reverse steps (at small
 // sizes neither kernel fills the GPU; a tile kernel's last round of tiles
-// leaves most SMs idle). The order the single-stream plan implies is kept by
-// events: a reverse step waits for the stage step that wrote its set; a stage
-// step waits until the reverse step that read the set it overwrites is done;
-// an advance that overwrites a slot a reverse step issued before still reads
-// waits for the reverse steps issued so far. Both streams run the same
-// launches as run_plan, so the results are identical. Must be called inside a
-// stream capture of the context's stream; set 0 (s1..s3) holds the stage
-// states of the plan's first reverse step on entry.
+// leaves most SMs idle). Both streams run the launches of run_plan on the same
+// states, so the results are identical.
+//
+// Write-after-read hazards: a stage step waits until the reverse step that
+// read the set it overwrites is done. An advance must not overwrite a state
+// that a reverse step issued before it still reads; in the binomial plan the
+// next advance after a segment's reversal writes the very slot that segment's
+// last reverse step reads (the slot it just released), so waiting there would
+// leave M idle for the whole advance. Instead the logical slots are renamed
+// onto physical buffers (the plan's slots, the work slot and kSpareSlots
+// spares): an advance whose target buffer still has a reader in flight writes
+// the spare read longest ago, which takes over the logical slot, and the old
+// buffer becomes a spare. R waits on a ring of per-reverse-step events
+// (recorded on M after each reverse step) only when the buffer it is about to
+// write has a reader that R has not yet waited for; a ring entry recorded again
+// by a later reverse step only makes a wait stronger, since M runs in order.
+// Reads of the renamed slots (advances, stage steps, reverse steps) follow the
+// mapping at their place in the plan, which every replay of the captured graph
+// repeats from the same identity mapping (the forward part writes the
+// checkpoints to the plan's own slots). Must be called inside a stream capture
+// of the context's stream; set 0 (s1..s3) holds the stage states of the plan's
+// first reverse step on entry.
 cudaError_t run_plan_overlapped(vt_ctx* c, size_t begin, size_t end) {
   AdjointState* s = c->adj;
   cudaStream_t M = c->stream, R = s->side;
   double2* const sets[2][3] = {{s->s1, s->s2, s->s3}, {s->t1, s->t2, s->t3}};
   bool ready_rec[2] = {false, false};  // ev_ready[k] recorded in this capture
-  bool freed_rec[2] = {false, false};  // ev_freed[k] recorded (a reverse step read set k)
+  long long set_reader[2] = {-1, -1};  // the reverse step that last read set k
   int cur = 0;                         // the set the last stage step wrote
-  int last_read = -1;                  // the set of the last reverse step issued, or -1
-  std::vector<long long> pending;      // slots read by reverse steps since R last waited for M
+  // physical buffers: the plan's slots 0..nlog-1, the work slot (logical nlog), the spares
+  const int nlog = s->plan_slots;
+  std::vector<double2*> buf;
+  for (int i = 0; i < nlog; ++i) buf.push_back(slot(c, i));
+  buf.push_back(s->work);
+  for (int i = 0; i < kSpareSlots; ++i) buf.push_back(slot(c, nlog + i));
+  std::vector<int> map(static_cast<size_t>(nlog) + 1);
+  for (int i = 0; i <= nlog; ++i) map[i] = i;
+  std::vector<int> spares;
+  for (int i = 0; i < kSpareSlots; ++i) spares.push_back(nlog + 1 + i);
+  std::vector<long long> last_read(buf.size(), -1);  // last reverse step reading each buffer
+  long long issued = 0;  // reverse steps issued on M
+  long long synced = 0;  // R has waited for every reverse step below this index
+  auto logical = [&](int sl) { return sl == kWorkSlot ? nlog : sl; };
+  auto wait_reverse = [&](long long k) -> cudaError_t {  // R waits until reverse step k is done
+    if (k < synced) return cudaSuccess;
+    synced = k + 1;
+    return cudaStreamWaitEvent(R, s->ev_rev[k % kRevRing], 0);
+  };
   cudaError_t e = cudaEventRecord(s->ev_fork, M);
   if (!e) e = cudaStreamWaitEvent(R, s->ev_fork, 0);
   for (size_t i = begin; i < end && !e; ++i) {
     const CkptAction& a = s->plan[i];
     switch (a.op) {
-      case CkptOp::kAdvance:
-        if (last_read >= 0 && std::find(pending.begin(), pending.end(), static_cast<long long>(a.dst)) != pending.end()) {
-          e = cudaStreamWaitEvent(R, s->ev_freed[last_read], 0);
-          pending.clear();
+      case CkptOp::kAdvance: {
+        const int ps = map[logical(a.src)];
+        const int L = logical(a.dst);
+        int pd = map[L];
+        if (last_read[pd] >= synced && !spares.empty()) {
+          size_t best = 0;
+          for (size_t j = 1; j < spares.size(); ++j)
+            if (last_read[spares[j]] < last_read[spares[best]]) best = j;
+          const int q = spares[best];
+          spares[best] = pd;
+          map[L] = pd = q;
         }
-        if (!e) e = advance(c, slot(c, a.src), a.steps, slot(c, a.dst), s->dt, R);
+        if (last_read[pd] >= synced) e = wait_reverse(last_read[pd]);
+        if (!e) e = advance(c, buf[ps], a.steps, buf[pd], s->dt, R);
         break;
+      }
       case CkptOp::kStageStep: {
         const int w = cur ^ 1;
-        if (freed_rec[w]) e = cudaStreamWaitEvent(R, s->ev_freed[w], 0);
-        if (!e) e = stage_step(c, slot(c, a.src), sets[w][0], sets[w][1], sets[w][2], s->dt, nullptr, R, true);
+        if (set_reader[w] >= 0) e = wait_reverse(set_reader[w]);
+        if (!e)
+          e = stage_step(c, buf[map[logical(a.src)]], sets[w][0], sets[w][1], sets[w][2], s->dt, nullptr, R, true);
         if (!e) e = cudaEventRecord(s->ev_ready[w], R);
         ready_rec[w] = true;
         cur = w;
         break;
       }
-      case CkptOp::kAdjoint:
+      case CkptOp::kAdjoint: {
+        const int pr = map[logical(a.src)];
         if (ready_rec[cur]) e = cudaStreamWaitEvent(M, s->ev_ready[cur], 0);
-        if (!e) e = adjoint_step(c, slot(c, a.src), sets[cur][0], sets[cur][1], sets[cur][2], s->dt);
-        if (!e) e = cudaEventRecord(s->ev_freed[cur], M);
-        freed_rec[cur] = true;
-        last_read = cur;
-        pending.push_back(a.src);
+        if (!e) e = adjoint_step(c, buf[pr], sets[cur][0], sets[cur][1], sets[cur][2], s->dt);
+        if (!e) e = cudaEventRecord(s->ev_rev[issued % kRevRing], M);
+        last_read[pr] = issued;
+        set_reader[cur] = issued;
+        ++issued;
         break;
+      }
     }
   }
   // the side stream rejoins the capture's origin stream
@@ -591,7 +646,9 @@ int vt_adjoint_forward(vt_ctx* c, double dt, int nsteps, int nsnapshots) {
   while (s->plan[s->first_adjoint].op != vt::CkptOp::kAdjoint) ++s->first_adjoint;
   for (const vt::CkptAction& a : s->plan)
     if (a.op == vt::CkptOp::kAdvance && a.dst != vt::kWorkSlot) used = std::max(used, a.dst + 1);
-  if ((st = vt::ensure_slots(c, used))) return st;
+  // the overlapped reverse sweep's spare buffers follow the plan's slots
+  s->plan_slots = used;
+  if ((st = vt::ensure_slots(c, used + vt::kSpareSlots))) return st;
   if ((st = vt_checkpoint_plan(nsteps, S, &s->info))) return st;
   cudaError_t e = vt::reset_error_words(c);
   if (!e)
