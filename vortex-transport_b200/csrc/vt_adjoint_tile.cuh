@@ -29,7 +29,9 @@
 //   5. flux^T the transposed nodal flux Jacobian of every node (its state in
 //             shared memory), once; the state tile is then free and the next
 //             tile's copies are issued;
-//   6. combine acc_out = acc_in + lam_coef lam + g, a_out = cl lam + cg g.
+//   6. combine acc_out = acc_in + lam_coef lam + g, a_out = cl lam + cg g,
+//             thread (element, component pair, node half) after the
+//             components of g meet in shared memory.
 //
 // As in the stage kernel, from phase 4 on every shared-memory access stays
 // within an element's four threads, so the barriers after phases 4a, 4b and 5
@@ -63,11 +65,6 @@ struct AdjTileLayout {
   static constexpr int kA = (kLF + 3 * NP * NFQ * 8 + 127) / 128 * 128;  // double2 [2][2NP][32] stage adjoint
   static constexpr int kBytes = kA + 2 * 2 * NP * kTileRun * 16;
 };
-
-// component c of node i of an SoA double2 state, element e
-__device__ __forceinline__ long long comp_index(long long KP, int i, int c, int e) {
-  return ((2 * i + (c >> 1)) * KP + e) * 2 + (c & 1);
-}
 
 // Lane 0 of warp `which` announces its run's two boxes (stage state and stage
 // adjoint) on the tile's mbarrier and issues both tensor copies.
@@ -410,32 +407,47 @@ __global__ void __launch_bounds__(4 * kTileElems, 2) adjoint_tile_kernel(const _
     }
     cp_async_commit();
 
-    // ---- 6. reverse RK combine, component c of every node ------------------------------
+    // ---- 6. reverse RK combine -------------------------------------------------------------
+    // the thread's component adjoints meet their pair partner's in shared memory
+    // (rows i*8 + c of the flux^T buffer, own column), then thread (el, h, half)
+    // combines component pair h of half of the nodes with 16-byte accesses, as
+    // the stage kernel's pair mapping does: half the load and store
+    // instructions of a per-component combine, on whole 16-byte pairs
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      const double gi = P > 0 ? g[i] + Gs[(i * 8 + c) * ES + el] : g[i];
+      Gs[(i * 8 + c) * ES + el] = gi;
+    }
+    run_sync(t);
     if (valid) {
-      const double h = a.elem_dt ? __ldg(a.elem_dt + e) : 1.0;
-      const double cl = a.elem_dt ? a.cl * h : a.cl, cg = a.elem_dt ? a.cg * h : a.cg;
+      constexpr int NH = (NP + 1) / 2;
+      const int h = grp & 1, half = grp >> 1;
+      const double hh = a.elem_dt ? __ldg(a.elem_dt + e) : 1.0;
+      const double cl = a.elem_dt ? a.cl * hh : a.cl, cg = a.elem_dt ? a.cg * hh : a.cg;
       const bool need_lam = a.lam_coef != 0.0 || a.a_out;
-      const double* lamp = reinterpret_cast<const double*>(a.lam);
-      const double* accp = reinterpret_cast<const double*>(a.acc_in);
-      double* acco = reinterpret_cast<double*>(a.acc_out);
-      double* aout = reinterpret_cast<double*>(a.a_out);
       // every load before the first store: acc_in and acc_out are the same
       // array in three of the four reverse stages, so loads that follow a
       // store could not be moved above it and each would wait on its own
-      // round trip to L2 (this phase took a quarter of the kernel's time)
-      double lv[NP], av[NP];
+      // round trip to L2
+      double2 lv[NH], av[NH];
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        const long long x = comp_index(KP, i, c, e);
-        lv[i] = need_lam ? lamp[x] : 0.0;
-        av[i] = accp ? accp[x] : 0.0;
+      for (int k = 0; k < NH; ++k) {
+        const int i = half * NH + k;
+        if (i < NP) {
+          const long long x = (2 * i + h) * KP + e;
+          lv[k] = need_lam ? a.lam[x] : make_double2(0.0, 0.0);
+          av[k] = a.acc_in ? a.acc_in[x] : make_double2(0.0, 0.0);
+        }
       }
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        const long long x = comp_index(KP, i, c, e);
-        const double gi = P > 0 ? g[i] + Gs[(i * 8 + c) * ES + el] : g[i];
-        acco[x] = fma(a.lam_coef, lv[i], av[i]) + gi;
-        if (aout) aout[x] = fma(cl, lv[i], cg * gi);
+      for (int k = 0; k < NH; ++k) {
+        const int i = half * NH + k;
+        if (i < NP) {
+          const long long x = (2 * i + h) * KP + e;
+          const double2 gi = make_double2(Gs[(i * 8 + 2 * h) * ES + el], Gs[(i * 8 + 2 * h + 1) * ES + el]);
+          a.acc_out[x] = make_double2(fma(a.lam_coef, lv[k].x, av[k].x) + gi.x, fma(a.lam_coef, lv[k].y, av[k].y) + gi.y);
+          if (a.a_out) a.a_out[x] = make_double2(fma(cl, lv[k].x, cg * gi.x), fma(cl, lv[k].y, cg * gi.y));
+        }
       }
     }
     // the four warps of a run hold different components of the same elements:
