@@ -433,10 +433,12 @@ cudaError_t run_plan(vt_ctx* c, size_t begin, size_t end, double2* out_last) {
 // onto physical buffers (the plan's slots, the work slot and kSpareSlots
 // spares): an advance whose target buffer still has a reader in flight writes
 // the spare read longest ago, which takes over the logical slot, and the old
-// buffer becomes a spare. R waits on a ring of per-reverse-step events
-// (recorded on M after each reverse step) only when the buffer it is about to
-// write has a reader that R has not yet waited for; a ring entry recorded again
-// by a later reverse step only makes a wait stronger, since M runs in order.
+// buffer becomes a spare (schedule_overlapped, vt_checkpoint.cpp, makes these
+// decisions on the host; a CPU test checks them on whole plans). R waits on a
+// ring of per-reverse-step events (recorded on M after each reverse step) only
+// when the buffer it is about to write has a reader that R has not yet waited
+// for; a ring entry recorded again by a later reverse step only makes a wait
+// stronger, since M runs in order.
 // Reads of the renamed slots (advances, stage steps, reverse steps) follow the
 // mapping at their place in the plan, which every replay of the captured graph
 // repeats from the same identity mapping (the forward part writes the
@@ -448,68 +450,31 @@ cudaError_t run_plan_overlapped(vt_ctx* c, size_t begin, size_t end) {
   cudaStream_t M = c->stream, R = s->side;
   double2* const sets[2][3] = {{s->s1, s->s2, s->s3}, {s->t1, s->t2, s->t3}};
   bool ready_rec[2] = {false, false};  // ev_ready[k] recorded in this capture
-  long long set_reader[2] = {-1, -1};  // the reverse step that last read set k
-  int cur = 0;                         // the set the last stage step wrote
-  // physical buffers: the plan's slots 0..nlog-1, the work slot (logical nlog), the spares
+  // physical buffers: the plan's slots 0..nlog-1, the work slot (nlog), the spares
   const int nlog = s->plan_slots;
   std::vector<double2*> buf;
   for (int i = 0; i < nlog; ++i) buf.push_back(slot(c, i));
   buf.push_back(s->work);
   for (int i = 0; i < kSpareSlots; ++i) buf.push_back(slot(c, nlog + i));
-  std::vector<int> map(static_cast<size_t>(nlog) + 1);
-  for (int i = 0; i <= nlog; ++i) map[i] = i;
-  std::vector<int> spares;
-  for (int i = 0; i < kSpareSlots; ++i) spares.push_back(nlog + 1 + i);
-  std::vector<long long> last_read(buf.size(), -1);  // last reverse step reading each buffer
-  long long issued = 0;  // reverse steps issued on M
-  long long synced = 0;  // R has waited for every reverse step below this index
-  auto logical = [&](int sl) { return sl == kWorkSlot ? nlog : sl; };
-  auto wait_reverse = [&](long long k) -> cudaError_t {  // R waits until reverse step k is done
-    if (k < synced) return cudaSuccess;
-    synced = k + 1;
-    return cudaStreamWaitEvent(R, s->ev_rev[k % kRevRing], 0);
-  };
+  const std::vector<OverlapStep> sched = schedule_overlapped(s->plan, begin, end, nlog, kSpareSlots);
   cudaError_t e = cudaEventRecord(s->ev_fork, M);
   if (!e) e = cudaStreamWaitEvent(R, s->ev_fork, 0);
-  for (size_t i = begin; i < end && !e; ++i) {
-    const CkptAction& a = s->plan[i];
-    switch (a.op) {
-      case CkptOp::kAdvance: {
-        const int ps = map[logical(a.src)];
-        const int L = logical(a.dst);
-        int pd = map[L];
-        if (last_read[pd] >= synced && !spares.empty()) {
-          size_t best = 0;
-          for (size_t j = 1; j < spares.size(); ++j)
-            if (last_read[spares[j]] < last_read[spares[best]]) best = j;
-          const int q = spares[best];
-          spares[best] = pd;
-          map[L] = pd = q;
-        }
-        if (last_read[pd] >= synced) e = wait_reverse(last_read[pd]);
-        if (!e) e = advance(c, buf[ps], a.steps, buf[pd], s->dt, R);
+  for (size_t i = 0; i < sched.size() && !e; ++i) {
+    const OverlapStep& x = sched[i];
+    if (x.wait >= 0) e = cudaStreamWaitEvent(R, s->ev_rev[x.wait % kRevRing], 0);
+    if (e) break;
+    switch (x.op) {
+      case CkptOp::kAdvance: e = advance(c, buf[x.src], x.steps, buf[x.dst], s->dt, R); break;
+      case CkptOp::kStageStep:
+        e = stage_step(c, buf[x.src], sets[x.set][0], sets[x.set][1], sets[x.set][2], s->dt, nullptr, R, true);
+        if (!e) e = cudaEventRecord(s->ev_ready[x.set], R);
+        ready_rec[x.set] = true;
         break;
-      }
-      case CkptOp::kStageStep: {
-        const int w = cur ^ 1;
-        if (set_reader[w] >= 0) e = wait_reverse(set_reader[w]);
-        if (!e)
-          e = stage_step(c, buf[map[logical(a.src)]], sets[w][0], sets[w][1], sets[w][2], s->dt, nullptr, R, true);
-        if (!e) e = cudaEventRecord(s->ev_ready[w], R);
-        ready_rec[w] = true;
-        cur = w;
+      case CkptOp::kAdjoint:
+        if (ready_rec[x.set]) e = cudaStreamWaitEvent(M, s->ev_ready[x.set], 0);
+        if (!e) e = adjoint_step(c, buf[x.src], sets[x.set][0], sets[x.set][1], sets[x.set][2], s->dt);
+        if (!e) e = cudaEventRecord(s->ev_rev[x.index % kRevRing], M);
         break;
-      }
-      case CkptOp::kAdjoint: {
-        const int pr = map[logical(a.src)];
-        if (ready_rec[cur]) e = cudaStreamWaitEvent(M, s->ev_ready[cur], 0);
-        if (!e) e = adjoint_step(c, buf[pr], sets[cur][0], sets[cur][1], sets[cur][2], s->dt);
-        if (!e) e = cudaEventRecord(s->ev_rev[issued % kRevRing], M);
-        last_read[pr] = issued;
-        set_reader[cur] = issued;
-        ++issued;
-        break;
-      }
     }
   }
   // the side stream rejoins the capture's origin stream

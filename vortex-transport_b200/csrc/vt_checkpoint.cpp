@@ -85,6 +85,71 @@ std::vector<CkptAction> plan_reversal(int n, int S) {
   return plan;
 }
 
+std::vector<OverlapStep> schedule_overlapped(const std::vector<CkptAction>& plan, size_t begin, size_t end,
+                                             int nlog, int nspare) {
+  std::vector<OverlapStep> out;
+  const int nbuf = nlog + 1 + nspare;
+  std::vector<int> map(static_cast<size_t>(nlog) + 1);  // logical slot (work slot = nlog) -> buffer
+  for (int i = 0; i <= nlog; ++i) map[i] = i;
+  std::vector<int> spares;
+  for (int i = 0; i < nspare; ++i) spares.push_back(nlog + 1 + i);
+  std::vector<long long> last_read(static_cast<size_t>(nbuf), -1);  // last reverse step reading each buffer
+  long long set_reader[2] = {-1, -1};  // the reverse step that last read each stage-state set
+  long long issued = 0;                // reverse steps scheduled
+  long long synced = 0;                // R has waited for every reverse step below this index
+  int cur = 0;                         // the set the last stage step wrote
+  auto logical = [&](int sl) { return sl == kWorkSlot ? nlog : sl; };
+  auto need = [&](long long k) -> long long {  // the wait R needs before it may overwrite what step k read
+    if (k < synced) return -1;
+    synced = k + 1;
+    return k;
+  };
+  for (size_t i = begin; i < end && i < plan.size(); ++i) {
+    const CkptAction& a = plan[i];
+    OverlapStep x{};
+    x.op = a.op;
+    x.step = a.step;
+    switch (a.op) {
+      case CkptOp::kAdvance: {
+        x.src = map[logical(a.src)];
+        const int L = logical(a.dst);
+        int pd = map[L];
+        if (last_read[pd] >= synced && !spares.empty()) {
+          size_t best = 0;
+          for (size_t j = 1; j < spares.size(); ++j)
+            if (last_read[spares[j]] < last_read[spares[best]]) best = j;
+          const int q = spares[best];
+          spares[best] = pd;
+          map[L] = pd = q;
+        }
+        x.dst = pd;
+        x.steps = a.steps;
+        x.wait = need(last_read[pd]);
+        break;
+      }
+      case CkptOp::kStageStep: {
+        const int w = cur ^ 1;
+        x.src = map[logical(a.src)];
+        x.set = w;
+        x.wait = need(set_reader[w]);
+        cur = w;
+        break;
+      }
+      case CkptOp::kAdjoint: {
+        x.src = map[logical(a.src)];
+        x.set = cur;
+        x.index = issued;
+        last_read[x.src] = issued;
+        set_reader[cur] = issued;
+        ++issued;
+        break;
+      }
+    }
+    out.push_back(x);
+  }
+  return out;
+}
+
 }  // namespace vt
 
 extern "C" int vt_checkpoint_plan(int nsteps, int nsnapshots, vt_checkpoint_info* out) {
