@@ -328,9 +328,12 @@ int vt_checkpoint_plan(int nsteps, int nsnapshots, vt_checkpoint_info* out);
 /* Forward sweep: nsteps RK4 steps of size dt from the current state, keeping
  * at most `nsnapshots` states in device memory (nsnapshots >= nsteps keeps
  * every step's start; >= 4 nsteps also every stage state, so the reverse
- * sweep recomputes nothing). On return the context holds U(T) exactly as
- * vt_step_rk4 would leave it and the time has advanced; a non-physical state
- * returns its code. */
+ * sweep recomputes nothing). Besides the snapshots the context holds eleven
+ * working state vectors, and a checkpointed sweep two more, onto which the
+ * reverse sweep renames slots so that its recomputation can run ahead of its
+ * reverse steps. On return the context holds U(T) exactly as vt_step_rk4
+ * would leave it and the time has advanced; a non-physical state returns its
+ * code. */
 int vt_adjoint_forward(vt_ctx* ctx, double dt, int nsteps, int nsnapshots);
 /* Reverse sweep of the last vt_adjoint_forward: given dJ/dU(T) returns
  * dJ/dU(0), recomputing the steps between checkpoints. Leaves the state and
