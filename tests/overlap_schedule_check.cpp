@@ -74,12 +74,9 @@ int check(int n, int S, int nspare, long long* waits_out) {
   int set_step[2] = {last_stage, -1};
   long long synced = 0;  // reverse steps below this index are known done on the side stream
   long long waits = 0;
-  // per buffer / set: reverse steps issued that read it and may still run (index, R position of their start)
-  struct Read {
-    long long index;
-  };
-  std::vector<std::vector<Read>> readers(static_cast<size_t>(nbuf));
-  std::vector<long long> set_last_reader = {-1, -1};
+  // per buffer: the reverse steps issued since its last write that read it
+  std::vector<std::vector<long long>> readers(static_cast<size_t>(nbuf));
+  long long set_last_reader[2] = {-1, -1};  // the last reverse step that read each set
   std::vector<int> seq_held = held;  // sequential model, continued through the reverse part
   long long next_index = 0;
   int expect_step = n - 1;
@@ -99,8 +96,8 @@ int check(int n, int S, int nspare, long long* waits_out) {
         const int want = seq_held[logical(a.src)];
         if (want < 0 || content[x.src] != want) return bad(n, S, nspare, i, "advance reads the wrong state");
         // write-after-read: every reverse step that read this buffer is done
-        for (const Read& r : readers[x.dst])
-          if (r.index >= synced) return bad(n, S, nspare, i, "advance overwrites a buffer a reverse step may still read");
+        for (const long long r : readers[x.dst])
+          if (r >= synced) return bad(n, S, nspare, i, "advance overwrites a buffer a reverse step may still read");
         readers[x.dst].clear();
         content[x.dst] = want + a.steps;
         seq_held[logical(a.dst)] = want + a.steps;
@@ -123,7 +120,7 @@ int check(int n, int S, int nspare, long long* waits_out) {
         if (set_step[x.set] != a.step) return bad(n, S, nspare, i, "reverse step reads another step's stage states");
         if (content[x.src] != a.step || seq_held[logical(a.src)] != a.step)
           return bad(n, S, nspare, i, "reverse step reads the wrong start state");
-        readers[x.src].push_back({next_index});
+        readers[x.src].push_back(next_index);
         set_last_reader[x.set] = next_index;
         ++next_index;
         break;
