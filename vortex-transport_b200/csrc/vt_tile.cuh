@@ -264,6 +264,17 @@ __device__ __forceinline__ void pair_volume(const StageOps<P, NFQ>& ops, const d
   }
 }
 
+// Stage 3's U3 / (3 c_out) (f = 1 / (3 c_out)) added to pair h of this half's
+// node accumulators, from the state tile.
+template <int P, int HALF>
+__device__ __forceinline__ void pair_fold(const double2* S, int h, int el, double f, double2* r) {
+  constexpr int NP = np_of_p(P), NH = (NP + 1) / 2, base = HALF * NH;
+#pragma unroll
+  for (int i = 0; i < NH; ++i)
+    if (base + i < NP) r[i] = make_double2(fma(f, S[sidx<NP>(2 * (base + i) + h, el)].x, r[i].x),
+                                           fma(f, S[sidx<NP>(2 * (base + i) + h, el)].y, r[i].y));
+}
+
 // Non-coherent loads issued where they are written, so that the stage
 // update's first operand is in flight during the volume phase (the compiler
 // would otherwise sink them to their use). They do not allocate in L1: three
@@ -281,9 +292,25 @@ __device__ __forceinline__ double2 ld_early2(const double2* p) {
   return v;
 }
 
+// The RK4 step in 12 state-vector passes. Classical RK4 (Timestepping.cpp:85-306)
+// with k_i the right-hand side at stage i's input has the stage states
+// U1 = U + dt/2 k1, U2 = U + dt/2 k2, U3 = U + dt k3, and since
+// dt/6 k1 = (U1 - U)/3 and dt/3 k3 = (U3 - U)/3 its new state is
+// X + U3/3 + dt/6 k4 with X = (U + U1)/3 + dt/3 k2:
+//   stage 0: reads U,              writes U1
+//   stage 1: reads U1, U (and U1 again from L2), writes U2 and X
+//   stage 2: reads U2, U,          writes U3
+//   stage 3: reads U3, X,          writes U_{n+1}
+// against 16 passes when the accumulator is carried through every stage. The
+// stage states are formed as before, bit for bit; only the last stage's sum is
+// grouped differently (rounding level). Stage 3 adds U3/3 by starting its
+// accumulators at U3/(3 c_out) while the state tile is still in shared memory.
+// The coefficient ratios are classical RK4's: (dt/6)/(dt/2) = (dt/3)/dt = 1/3.
+constexpr double kThird = 1.0 / 3.0;
+
 // The stage's read-only operand that the update needs besides the
-// accumulator: U_n (stage 0, forward Euler), the accumulator (stage 3) or
-// the base U_n (stages 1, 2); none for the bare right-hand side.
+// accumulator: U_n (stage 0, forward Euler), X (stage 3) or the base U_n
+// (stages 1, 2); none for the bare right-hand side.
 __device__ __forceinline__ const double2* first_operand(const StageArgs& a) {
   return (a.stage == 0 || a.stage == kStageEuler) ? a.in : (a.stage == 3 ? a.acc : a.base);
 }
@@ -305,34 +332,28 @@ __device__ __forceinline__ void pair_update(const StageArgs& a, int e, int h, do
   const long long o = (2 * HALF * NH + h) * KP + e;  // row 2 * node + h of this half's first node
   constexpr int N = NP - HALF * NH < NH ? NP - HALF * NH : NH;  // nodes of this half
   switch (a.stage) {
-    case 0:
+    case 1: {
       if (!a.no_acc) {
+        // X = (U_n + U1) / 3 + c_acc k2, U1 being this stage's input, re-read
+        // here (its tile was copied one tile ago and is still in L2) by loads
+        // that stay where they are written (plain loads of the read-only
+        // input were hoisted and spilled); every row is read before the first
+        // store, since a load that follows a store to another array cannot be
+        // moved above it
+        double2 iv[NH];
 #pragma unroll
-        for (int i = 0; i < N; ++i) __stcs(a.acc + (o + i * 2 * KP), fma2(c_acc, r[i], pre[i]));
+        for (int i = 0; i < N; ++i) iv[i] = ld_early2(a.in + o + i * 2 * KP);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+          __stcs(a.acc + (o + i * 2 * KP),
+                 fma2(c_acc, r[i], make_double2((pre[i].x + iv[i].x) * kThird, (pre[i].y + iv[i].y) * kThird)));
       }
 #pragma unroll
       for (int i = 0; i < N; ++i) __stcs(a.out + (o + i * 2 * KP), fma2(c_out, r[i], pre[i]));
       break;
-    case 1:
-    case 2: {
-      if (a.no_acc) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) __stcs(a.out + (o + i * 2 * KP), fma2(c_out, r[i], pre[i]));
-        break;
-      }
-      // every accumulator row is read before the first store: a load that
-      // follows a store to another array cannot be moved above it, so read
-      // and written in turn each row would wait on its own memory round trip
-      double2 av[NH];
-#pragma unroll
-      for (int i = 0; i < N; ++i) av[i] = a.acc[o + i * 2 * KP];
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        __stcs(a.acc + (o + i * 2 * KP), fma2(c_acc, r[i], av[i]));
-        __stcs(a.out + (o + i * 2 * KP), fma2(c_out, r[i], pre[i]));
-      }
-      break;
     }
+    case 0:
+    case 2:
     case 3:
     case kStageEuler:
 #pragma unroll
@@ -434,7 +455,7 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
       const int which = t & 1, vec = (t - 64) >> 1;  // vec 0: acc, 1: base
       const int start = which ? run.z : run.x, len = which ? run.w : run.y;
       if (len > 0) {
-        if (vec == 0 && a.stage >= 1 && a.stage <= 3 && !a.no_acc) tensor_prefetch_l2(&a.map_acc, 2 * start, 0);
+        if (vec == 0 && a.stage == 3) tensor_prefetch_l2(&a.map_acc, 2 * start, 0);
         if (vec == 1 && (a.stage == 1 || a.stage == 2)) tensor_prefetch_l2(&a.map_base, 2 * start, 0);
       }
     } else if (t >= 64 + 8 * NP && t < 64 + 8 * NP + 56) {
@@ -606,6 +627,21 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
         }
       }
     }
+    // stage 3: U3 / (3 c_out) into the accumulators while the state tile still
+    // holds U3 (the update then writes X + c_out (k4 + U3 / (3 c_out)))
+    if (a.stage == 3 && valid) {
+      const double dtt = a.tile_dt ? __ldg(a.tile_dt + tile) : 1.0;
+      const double f = kThird / (a.c_out * dtt);
+      if constexpr (PAIR) {
+        if (grp >> 1) pair_fold<P, 1>(S, grp & 1, el, f, r2);
+        else pair_fold<P, 0>(S, grp & 1, el, f, r2);
+      } else {
+        const int c = grp;
+        const double* Sd = reinterpret_cast<const double*>(S);
+#pragma unroll
+        for (int i = 0; i < NP; ++i) r[i] = fma(f, Sd[sidx<NP>(2 * i + (c >> 1), el) * 2 + (c & 1)], r[i]);
+      }
+    }
     (void)NR;
     run_sync(t);
 
@@ -715,31 +751,21 @@ __global__ void __launch_bounds__(4 * kTileElems, 3) tile_stage_kernel(const __g
         double* out = reinterpret_cast<double*>(a.out) + off0;
         const long long step = 4 * KP;  // doubles between node rows of the same pair
         switch (a.stage) {
-          case 0:
-            if (!a.no_acc) {
+          case 1: {
+            if (!a.no_acc) {  // X = (U_n + U1) / 3 + c_acc k2, as in pair_update
+              const double* in = reinterpret_cast<const double*>(a.in) + off0;
+              double iv[NP];  // all reads before the first store
 #pragma unroll
-              for (int i = 0; i < NP; ++i) __stcs(acc + i * step, fma(c_acc, r[i], pre[i]));
+              for (int i = 0; i < NP; ++i) iv[i] = ld_early(in + i * step);
+#pragma unroll
+              for (int i = 0; i < NP; ++i) __stcs(acc + i * step, fma(c_acc, r[i], (pre[i] + iv[i]) * kThird));
             }
 #pragma unroll
             for (int i = 0; i < NP; ++i) __stcs(out + i * step, fma(c_out, r[i], pre[i]));
             break;
-          case 1:
-          case 2: {
-            if (a.no_acc) {
-#pragma unroll
-              for (int i = 0; i < NP; ++i) __stcs(out + i * step, fma(c_out, r[i], pre[i]));
-              break;
-            }
-            double av[NP];  // all reads before the first store, as in pair_update
-#pragma unroll
-            for (int i = 0; i < NP; ++i) av[i] = acc[i * step];
-#pragma unroll
-            for (int i = 0; i < NP; ++i) {
-              __stcs(acc + i * step, fma(c_acc, r[i], av[i]));
-              __stcs(out + i * step, fma(c_out, r[i], pre[i]));
-            }
-            break;
           }
+          case 0:
+          case 2:
           case 3:
           case kStageEuler:
 #pragma unroll
