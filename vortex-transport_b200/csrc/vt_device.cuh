@@ -61,7 +61,7 @@ struct StageOps {
 struct StageArgs {
   const double2* in;    // state the right-hand side is evaluated on
   const double2* base;  // U_n (RK4 stages 1, 2)
-  double2* acc;         // RK4 accumulator
+  double2* acc;         // RK4 accumulator X (written by stage 1, read by stage 3; vt_tile.cuh)
   double2* out;         // next stage state / new U / the right-hand side itself
   const double2* geo;
   const int4* nbr;
@@ -74,7 +74,7 @@ struct StageArgs {
   int K;
   int ntiles;
   int stage;     // 0..3 RK4 stages, 4 forward Euler, 5 right-hand side only
-  double c_acc;  // accumulator coefficient
+  double c_acc;  // accumulator coefficient (stage 1)
   double c_out;  // output coefficient
   // Test hook of the bounded waits (vt_test_bulk_wait): polls of the tile's
   // mbarrier before a wait gives up (0: the default bound), and bit 0 of
@@ -82,7 +82,7 @@ struct StageArgs {
   unsigned wait_tries = 0;
   int test_flags = 0;
   // RK4 stages 0-2 that only produce the next stage state (a step rerun to
-  // keep its stage states): the accumulator is neither read nor written
+  // keep its stage states): stage 1 does not form the accumulator
   int no_acc = 0;
   // 2-D tensor maps of in / acc / base, [2 Np rows] x [2 Kpad doubles], box of
   // 2 Np rows x 64 doubles (one 32-element run); encoded on the host by the
