@@ -332,7 +332,7 @@ cudaError_t advance(vt_ctx* c, const double2* X, int k, double2* Y, double dt, c
 // Step from X keeping the stage states in S1, S2, S3; the new state goes to
 // `out` when given (else the last stage is not run). With no_acc (only when
 // no last stage will follow on this accumulator: the reverse sweeps' reruns)
-// stages 0-2 neither read nor write the accumulator.
+// stage 1 does not form the accumulator (stages 0 and 2 never touch it).
 cudaError_t stage_step(vt_ctx* c, const double2* X, double2* S1, double2* S2, double2* S3, double dt0,
                        double2* out, cudaStream_t st, bool no_acc = false) {
   const double dt = dt_scale(c, dt0);
