@@ -277,7 +277,9 @@ __device__ __forceinline__ void pair_fold(const double2* S, int h, int el, doubl
 
 // Non-coherent loads issued where they are written, so that the stage
 // update's first operand is in flight during the volume phase (the compiler
-// would otherwise sink them to their use). They do not allocate in L1: three
+// would otherwise sink them to their use), and so that stage 1's re-read of
+// its input stays in the update (plain loads were hoisted and spilled). They
+// do not allocate in L1: three
 // 73 KB blocks leave about 30 KB of it, which the tile's geometry rows and the
 // face phase's neighbour rows use, and each operand row is read once (0.2%
 // faster at 768 x 768, p = 3).
